@@ -1,0 +1,364 @@
+"""Benchmark of the packed-Pauli hot path (one JSON line on rank 0).
+
+Default workload (N=1): config 2 of the reference's benchmark set --
+A (32,768 terms) x B (16,384 terms) on 100 qubits, k-local weight {2,3,4},
+then simplify (atol=1e-12): 536,870,912 products.  Metric: products simplified
+per second ("terms/s").  Other workloads: --workload commutation (config 3,
+bit-packed 262,144^2 matrix), expectation (config 4, forward + gradient),
+batched (config 5), plain (config 1 sequence).
+
+* value      device-resident throughput; each step is timed with CUDA events on
+             the stream the library launches on, L2 flushed between steps;
+* e2e        the same metric through the public API (wolfgang_quantum.PauliSum
+             host objects: host->device upload of the operands, device->host
+             read of the result inside the timed region);
+* roofline   the dominant kernel of the step, from CUDA events recorded around
+             each launch by the library's profiler during the timed steps;
+* cpu_baseline  the reference's own C++ core (oracle/_ref, compiled from its
+             sources) on a bounded sample of the same workload, 1 core.
+`--impl reference` times that reference core alone as the reference arm.
+Multi-GPU (torchrun): every rank runs an independent replica (the path has no
+exchange step); value = all ranks' work / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks() -> tuple[float, str]:
+    try:
+        return float(json.loads(PEAKS_FILE.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- distributed
+
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- helpers
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)  # 512 MiB write, larger than the 126 MB L2
+
+
+def dev(torch, a):
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.uint64:
+        return torch.from_numpy(a.view(np.int64)).cuda()
+    return torch.from_numpy(a).cuda()
+
+
+def roofline(prof: dict, bytes_per_launch: dict, peak: float, peak_kind: str) -> dict:
+    """Dominant kernel by total time; achieved = its algorithmic bytes per launch / mean launch time."""
+    if not prof:
+        return {}
+    name, (count, total_ms) = max(prof.items(), key=lambda kv: kv[1][1])
+    per_launch_ms = total_ms / count
+    algo_bytes = bytes_per_launch.get(name)
+    out = {"kernel": name, "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_source": peak_kind,
+           "launches": count, "ms_per_launch": per_launch_ms, "traffic": None,
+           "share": total_ms / sum(v[1] for v in prof.values())}
+    if algo_bytes:
+        achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
+        out.update(achieved=achieved, frac=achieved / peak, algorithmic_bytes=algo_bytes)
+    return out
+
+
+# ---------------------------------------------------------------- products (config 2)
+
+def reference_products_sample(A, B, rows: int) -> tuple[float, int]:
+    """Reference PauliSum::matmul(simplify=True) on A[:rows] x B; returns (seconds, products)."""
+    from oracle import Reference
+
+    ref = Reference()
+    n, ax, az, ac = A
+    _, bx, bz, bc = B
+    t0 = time.perf_counter()
+    ref.matmul(n, (ax[:rows], az[:rows], ac[:rows]), (bx, bz, bc), simplify=True,
+               max_intermediate_terms=rows * len(bc))
+    return time.perf_counter() - t0, rows * len(bc)
+
+
+def bench_products(args, world, rank, torch) -> dict:
+    from wolfgang_b200 import capi
+    from wolfgang_b200.workloads import config2
+
+    A, B = config2()
+    n = A[0]
+    W = 2
+    nl, nr = len(A[3]), len(B[3])
+    P = nl * nr
+    ax, az, ac = dev(torch, A[1]), dev(torch, A[2]), dev(torch, A[3])
+    bx, bz, bc = dev(torch, B[1]), dev(torch, B[2]), dev(torch, B[3])
+    stream = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    L = capi.lib()
+    l2 = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    U_last = [0]
+
+    def step():
+        ox, oz, oc = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        U = ctypes.c_size_t()
+        capi.check(L.wg_pauli_products(0 if world == 1 else torch.cuda.current_device(), W, ax.data_ptr(),
+                                       az.data_ptr(), ac.data_ptr(), nl, bx.data_ptr(), bz.data_ptr(), bc.data_ptr(),
+                                       nr, capi.WG_PRODUCTS_SIMPLIFY, 1e-12, 0.0, ctypes.byref(ox), ctypes.byref(oz),
+                                       ctypes.byref(oc), ctypes.byref(U), sh))
+        U_last[0] = U.value
+        for p in (ox, oz, oc):
+            capi.check(L.wg_free(torch.cuda.current_device(), p, sh))
+
+    for _ in range(args.warmup):
+        step()
+        flush_l2(torch, l2)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = capi.kernel_launches()
+    capi.profile_enable(True)
+    capi.profile_report()
+    total_ms = 0.0
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            flush_l2(torch, l2)
+        torch.cuda.synchronize()
+    capi.profile_enable(False)
+    prof = capi.profile_report()
+    launches = capi.kernel_launches() - launches0
+    barrier(world)
+    torch.cuda.synchronize()
+    t_max = max_over_ranks(total_ms, world)
+    ms_per_step = t_max / args.steps
+    value = world * P / (ms_per_step * 1e-3)
+    U = U_last[0]
+
+    # roofline: algorithmic bytes per launch of each kernel (the bytes a launch
+    # must move at minimum): keys are 2W words + a 4-byte index per item.
+    rec = 8 * 2 * W + 4
+    per_launch = {
+        "products_kernel": P * (rec + 16),                    # write keys+index+coefficient
+        "radix_scatter_kernel": P * 2 * rec,                  # read + write keys and index
+        "radix_hist_kernel": P * 8,                           # read one key word
+        "seg_head_kernel": P * (8 * 2 * W + 4),               # read keys, write flag
+        "seg_reduce_kernel": P * (4 + 16) + U * 20,           # idx + gathered coefficient, sums
+        "write_out_kernel": U * (8 * 2 * W + 16),
+    }
+    peak, peak_kind = peaks()
+    out = {
+        "metric": "H@H+simplify terms/s",
+        "value": value,
+        "unit": "terms/s",
+        "ms_per_step": ms_per_step,
+        "config": {"workload": "config2: A(32768)xB(16384) terms, 100 qubits, k-local w in {2,3,4}, matmul+simplify(atol=1e-12)",
+                   "products": P, "survivors": U, "words": W,
+                   "l2": "intermediates >> L2 (126 MB); 512 MiB L2 flush between steps",
+                   "survey_bytes_per_step": 2 * P * 48 + U * 48,
+                   "survey_effective_GBps": (2 * P * 48 + U * 48) / (ms_per_step * 1e-3) / 1e9},
+        "roofline": roofline(prof, per_launch, peak, peak_kind),
+        "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+
+    # end to end through the public API (host PauliSum in, host PauliSum out)
+    if args.e2e_steps > 0:
+        import wolfgang_quantum as wq
+
+        hA = wq.PauliSum._from_packed(n, A[1], A[2], A[3])
+        hB = wq.PauliSum._from_packed(n, B[1], B[2], B[3])
+        hA.matmul(hB, max_intermediate_terms=P)  # warm
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            r = hA.matmul(hB, max_intermediate_terms=P)
+        dt = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, world)
+        out["e2e"] = {"value": world * P / dt, "unit": "terms/s", "s_per_step": dt,
+                      "h2d_bytes_per_step": (nl + nr) * (16 * W + 16),
+                      "d2h_bytes_per_step": r.num_terms * (16 * W + 16),
+                      "api": "wolfgang_quantum.PauliSum.matmul (host operands and result)"}
+        del r
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        secs, prods = reference_products_sample(A, B, args.cpu_rows)
+        out["cpu_baseline"] = {"value": prods / secs, "unit": "terms/s", "cores": 1, "kind": "reference",
+                               "sample": f"A[:{args.cpu_rows}] x B = {prods} products, reference PauliSum::matmul"
+                                         f"(simplify=True) compiled from its sources, {secs:.1f} s"}
+    return out
+
+
+def reference_arm(args, world, rank) -> dict:
+    """Times the reference's own CPU core on bounded samples of the same workload."""
+    from wolfgang_b200.workloads import config2
+
+    A, B = config2()
+    for _ in range(args.warmup):
+        reference_products_sample(A, B, 16)
+    total, prods = 0.0, 0
+    for _ in range(args.steps):
+        s, p = reference_products_sample(A, B, args.ref_rows)
+        total += s
+        prods += p
+    v = prods / total
+    return {
+        "metric": "H@H+simplify terms/s", "value": v, "unit": "terms/s", "impl": "reference",
+        "ms_per_step": 1e3 * total / args.steps,
+        "config": {"workload": "config2: A(32768)xB(16384) terms, 100 qubits, k-local w in {2,3,4}, matmul+simplify(atol=1e-12)",
+                   "sample_rows": args.ref_rows},
+        "cpu_baseline": {"value": v, "unit": "terms/s", "cores": 1, "kind": "reference",
+                         "sample": f"A[:{args.ref_rows}] x B per step ({args.ref_rows * len(B[3])} products), "
+                                   "reference PauliSum::matmul(simplify=True), scalar path, 1 core"},
+        "e2e": {"value": v, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["products"], default="products")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-rows", type=int, default=1024)
+    ap.add_argument("--ref-rows", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        out = reference_arm(args, 1, 0)
+        out.update(n_gpus=args.gpus, steps=args.steps, warmup=args.warmup, higher_is_better=True,
+                   scaling="weak", vs_baseline=None, dtype="f64", data="synthetic (seeded generator of config 2)")
+        print(json.dumps(out), flush=True)
+        return
+
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    out = bench_products(args, world, rank, torch)
+    out.update(n_gpus=world, steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling="weak",
+               vs_baseline=None, dtype="f64", data="synthetic (seeded generator of config 2)")
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

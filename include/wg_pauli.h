@@ -1,0 +1,205 @@
+/*
+ * wg_pauli.h -- C-ABI of the B200 (sm_100a) packed-Pauli kernels.
+ *
+ * This is the boundary between the host layers (the C++ drop-in classes of
+ * include/wolfgang/, the Python module, ctypes callers) and the CUDA kernels in
+ * libwgpauli.so.  Everything here is plain C: pointers, sizes, status codes.
+ * No exception crosses it, and no CUDA or torch type appears in it (streams are
+ * passed as the opaque wg_stream_t, which is the same pointer as cudaStream_t;
+ * NULL means the legacy default stream).
+ *
+ * Data layout (the reference's PauliSum storage, include/wolfgang/pauli_sum.hpp
+ * :125-138 of sghowell/wolfgang 0.2.3):
+ *   x[t*words + q/64] bit (q%64) = X part of qubit q of term t; z likewise;
+ *   I=00 X=10 Z=01 Y=11; words = ceil(num_qubits/64) (0 for 0 qubits);
+ *   coefficients are complex128 stored as interleaved (re, im) doubles.
+ * Device pointers must live on `device`.  Every entry point enqueues on
+ * `stream`; entry points that return host values synchronise that stream.
+ *
+ * Status: WG_OK (0) or an error code; wg_last_error() returns the thread's
+ * last message.  The C++ layer maps WG_ERR_INVALID to std::invalid_argument
+ * (Python ValueError) and the others to std::runtime_error.
+ */
+#ifndef WG_PAULI_H
+#define WG_PAULI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WG_OK 0
+#define WG_ERR_INVALID 1  /* bad argument (reference: std::invalid_argument) */
+#define WG_ERR_OOM 2      /* device memory exhausted */
+#define WG_ERR_CUDA 3     /* CUDA runtime failure */
+#define WG_ERR_TIMEOUT 4  /* a bounded device wait expired; the context stays usable */
+#define WG_ERR_NO_DEVICE 5
+
+#define WG_DTYPE_C128 0
+#define WG_DTYPE_C64 1
+
+typedef struct CUstream_st* wg_stream_t;
+
+/* ------------------------------------------------------------ runtime ---- */
+const char* wg_last_error(void);
+int wg_abi_version(void);
+/* Device discovery; replaces DevicePauliSum::cuda_status()
+ * (include/wolfgang/device_pauli_sum.hpp:111, src/cuda/device_pauli_sum.cu:286-335). */
+int wg_device_count(int* count);
+int wg_runtime_versions(int* runtime_version, int* driver_version);
+int wg_device_info(int ordinal, char* name, size_t name_cap, int* cc_major,
+                   int* cc_minor, size_t* total_mem, int* sm_count);
+
+/* ------------------------------------------------------------- memory ---- */
+/* Stream-ordered allocations from the device's memory pool; replace the
+ * per-call cudaMalloc/cudaFree of src/cuda/device_pauli_sum.cuh:70-113. */
+int wg_malloc(int device, size_t bytes, wg_stream_t stream, void** out);
+int wg_free(int device, void* ptr, wg_stream_t stream);
+int wg_memcpy_htod(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
+int wg_memcpy_dtoh(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
+int wg_memcpy_dtod(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
+int wg_memset(int device, void* dst, int value, size_t bytes, wg_stream_t stream);
+int wg_stream_synchronize(int device, wg_stream_t stream);
+int wg_device_synchronize(int device);
+/* Pointer validation for caller-owned statevectors; replaces the checks of
+ * src/cuda/expectation_cuda.cu:211-250: is_device = -1 when the runtime does
+ * not recognise the pointer, 0 for host memory, 1 for device memory; then
+ * *device is its ordinal and in_one_allocation says whether the byte range
+ * [ptr, ptr+bytes) lies in one allocation. */
+int wg_pointer_check(const void* ptr, size_t bytes, int* is_device, int* device,
+                     int* in_one_allocation);
+/* Host-side fault injection for tests: the n-th next pool allocation (counting
+ * from 1) reports WG_ERR_OOM without touching the device; n <= 0 disables. */
+int wg_inject_alloc_failure(long n);
+/* Number of kernels this library has launched in the process (all devices). */
+int wg_kernel_launches(unsigned long long* count);
+/* Per-kernel timing with CUDA events recorded on each kernel's launch stream
+ * (off by default).  The report is "name:launches:total_ms;..." for the
+ * kernels since the last report; it synchronises on the recorded events. */
+int wg_profile_enable(int on);
+int wg_profile_report(char* buf, size_t cap);
+
+/* -------------------------------------------------------- commutation ---- */
+/* Bit-packed all-pairs commutation matrix.  Replaces commutation_kernel
+ * (src/cuda/commutation_cuda.cu:123-151) behind DevicePauliSum::commutes_with*
+ * (include/wolfgang/device_pauli_sum.hpp:126-147) and PauliSum::commutes_with
+ * (include/wolfgang/pauli_sum.hpp:77-79).
+ * bits[row*pitch_words + c/32] bit (c%32) = 1 iff lhs term `row` commutes with
+ * rhs term c; pitch_words >= ceil(n_rhs/32); padding bits are written 0.
+ * algo: 0 = autotuned choice, 1 = popcount/LOP3 with warp-ballot packing,
+ * 2 = bit-plane XOR over the lhs support.  All algos give identical bits. */
+int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x,
+                        const uint64_t* lhs_z, size_t n_lhs, const uint64_t* rhs_x,
+                        const uint64_t* rhs_z, size_t n_rhs, uint32_t* bits,
+                        size_t pitch_words, int algo, wg_stream_t stream);
+/* Dense uint8 flags (the reference's layout: out[row*n_rhs + c] in {0,1}). */
+int wg_bits_to_u8(int device, const uint32_t* bits, size_t rows, size_t cols,
+                  size_t pitch_words, uint8_t* out, wg_stream_t stream);
+/* Popcount consumers over the bit matrix; replace the reductions of
+ * src/cuda/device_commutation_matrix.cu:84-141.  Any output may be NULL;
+ * row_counts[rows] / col_counts[cols] are device buffers, *total is host. */
+int wg_bits_count(int device, const uint32_t* bits, size_t rows, size_t cols,
+                  size_t pitch_words, uint64_t* row_counts, uint64_t* col_counts,
+                  uint64_t* total, wg_stream_t stream);
+/* The same counts over a dense uint8 flag matrix (DeviceCommutationMatrix). */
+int wg_u8_count(int device, const uint8_t* flags, size_t rows, size_t cols,
+                uint64_t* row_counts, uint64_t* col_counts, uint64_t* total,
+                wg_stream_t stream);
+
+/* ----------------------------------------------------------- simplify ---- */
+/* PauliSum::simplify semantics (include/wolfgang/pauli_sum.hpp:57,
+ * src/simplify.cpp:147-430); replaces src/cuda/simplify_cuda.cu:382-791.
+ * Duplicate keys are summed in input order, |sum| <= atol + rtol*max|c| is
+ * dropped, survivors come out in canonical order (x0,z0,x1,z1,...).  The
+ * output buffers are allocated by the library on `device` (release with
+ * wg_free); they are NULL when *out_terms == 0.  Synchronises `stream`. */
+int wg_simplify(int device, size_t words, size_t n_terms, const uint64_t* x,
+                const uint64_t* z, const double* coeffs, double atol, double rtol,
+                uint64_t** out_x, uint64_t** out_z, double** out_coeffs,
+                size_t* out_terms, wg_stream_t stream);
+
+/* All-pairs products lhs*rhs (rhs acts first), PauliSum::matmul semantics
+ * (include/wolfgang/pauli_sum.hpp:70-73, src/multiply.cpp:73-402); replaces
+ * matmul_product_kernel (src/cuda/matmul_cuda.cu:36-87) + simplify.
+ * mode: WG_PRODUCTS_RAW       products in nested-loop order (lhs outer);
+ *       WG_PRODUCTS_SIMPLIFY  then simplify(atol, rtol);
+ *       WG_PRODUCTS_FUSED     then sum and cull at |c| > 1e-12 (the threshold
+ *                             of the reference's fused hash path,
+ *                             src/multiply.cpp:107-261).
+ * Outputs are allocated by the library as for wg_simplify. */
+#define WG_PRODUCTS_RAW 0
+#define WG_PRODUCTS_SIMPLIFY 1
+#define WG_PRODUCTS_FUSED 2
+int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
+                      const uint64_t* lhs_z, const double* lhs_c, size_t n_lhs,
+                      const uint64_t* rhs_x, const uint64_t* rhs_z,
+                      const double* rhs_c, size_t n_rhs, int mode, double atol,
+                      double rtol, uint64_t** out_x, uint64_t** out_z,
+                      double** out_coeffs, size_t* out_terms, wg_stream_t stream);
+
+/* -------------------------------------------------------- expectation ---- */
+/* <psi|H|psi> (PauliSum::expectation_statevector_complex{128,64},
+ * include/wolfgang/pauli_sum.hpp:91-94; DevicePauliSum::expectation_statevector_*
+ * include/wolfgang/device_pauli_sum.hpp:117-125); replaces
+ * expectation_statevector_terms_kernel (src/cuda/expectation_cuda.cu:79-126).
+ * Terms are grouped by x-mask so one streaming pass over psi serves every term
+ * of a group.  An expectation plan holds the grouping for one operator
+ * (device copies of its terms); it can be reused for many statevectors.
+ * psi is a device buffer of 2^n_qubits complex128 or complex64 (FP64
+ * accumulation either way).  n_qubits <= 63. */
+typedef struct wg_expect_plan_s* wg_expect_plan_t;
+int wg_expect_plan_create(int device, size_t n_qubits, size_t n_terms,
+                          const uint64_t* x, const uint64_t* z, const double* coeffs,
+                          wg_expect_plan_t* plan, wg_stream_t stream);
+int wg_expect_plan_destroy(wg_expect_plan_t plan);
+/* Replaces the coefficients of a plan (same terms, new values; device buffer
+ * of 2*n_terms doubles in the plan's original term order). */
+int wg_expect_plan_set_coeffs(wg_expect_plan_t plan, const double* coeffs, wg_stream_t stream);
+int wg_expect_plan_info(wg_expect_plan_t plan, size_t* n_groups, size_t* n_terms);
+/* Forward and adjoint in one x-grouped pass.  Any output may be NULL:
+ *   result[2]        E = sum_k c_k <psi|P_k|psi> (device, complex128);
+ *   term_values[T]   e_k = <psi|P_k|psi> (device, real FP64, original order) = dE/dc_k;
+ *   hpsi[2^n]        H|psi> (device, complex128) = dE/dpsi* for Hermitian H. */
+int wg_expect_plan_run(wg_expect_plan_t plan, const void* psi, int psi_dtype,
+                       double* result, double* term_values, double* hpsi,
+                       wg_stream_t stream);
+/* One-shot drop-in: builds a plan, runs it, returns E on the host. */
+int wg_expectation(int device, size_t n_qubits, size_t n_terms, const uint64_t* x,
+                   const uint64_t* z, const double* coeffs, const void* psi,
+                   int psi_dtype, double* result_host, wg_stream_t stream);
+
+/* Batched uneven (H, psi) pairs in one persistent launch with a device work
+ * queue (new; no reference counterpart).  Pair p uses plans[p] and psis[p]
+ * (dtype psi_dtype for all pairs); outputs per pair as in wg_expect_plan_run
+ * (arrays of device pointers; an array may be NULL, an element may be NULL).
+ * The plan array and pointer arrays are host arrays. */
+int wg_expect_batched(int device, size_t n_pairs, const wg_expect_plan_t* plans,
+                      const void* const* psis, int psi_dtype, double* const* results,
+                      double* const* term_values, double* const* hpsis,
+                      wg_stream_t stream);
+
+/* <H> over computational-basis counts (PauliSum::expectation_z_counts,
+ * src/expectation.cpp:219-247): packed[rows*words] bitstrings (device),
+ * counts[rows] (device).  Diagonal terms only.  Result on the host. */
+int wg_expectation_z_counts(int device, size_t words, size_t n_terms,
+                            const uint64_t* x, const uint64_t* z, const double* coeffs,
+                            size_t rows, const uint64_t* packed, const double* counts,
+                            double* result_host, wg_stream_t stream);
+
+/* ------------------------------------------------------------ grouping ---- */
+/* PauliSum::group_commuting(mode, "largest_first") (include/wolfgang/pauli_sum.hpp
+ * :84-87, src/grouping.cpp:197-290): greedy first-fit over the deterministic
+ * order (weight desc, canonical key, index).  mode_full = 0 for "qwc",
+ * 1 for "full".  x/z are device buffers; order_out[n_terms] and
+ * sizes_out[n_terms] are host buffers receiving term indices group after group
+ * (placement order) and the group sizes. */
+int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t* x,
+                       const uint64_t* z, int mode_full, size_t* order_out,
+                       size_t* sizes_out, size_t* n_groups, wg_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WG_PAULI_H */

@@ -1,0 +1,425 @@
+// PauliSum host implementation.
+//
+// Storage, parsing, export and the O(T) arithmetic follow the reference's host
+// semantics (src/pauli_sum.cpp:14-43, src/parse.cpp:15-97, src/export.cpp:12-53,
+// src/arithmetic.cpp:14-57) with the same error messages.  Every compute method
+// uploads its operands and runs on the GPU through the wg_* C-ABI.
+
+#include "wolfgang/pauli_sum.hpp"
+
+#include <algorithm>
+#include <bit>
+#include <cmath>
+#include <complex>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <unordered_set>
+#include <utility>
+#include <vector>
+
+#include "abi.hpp"
+#include "guards.hpp"
+
+namespace wolfgang {
+
+using abi::DeviceBuffer;
+
+namespace {
+
+bool valid_pauli(char p) { return p == 'I' || p == 'X' || p == 'Y' || p == 'Z'; }
+
+void set_bit(std::vector<std::uint64_t>& v, std::size_t words, std::size_t term, std::size_t q) {
+  v[term * words + q / 64] |= std::uint64_t{1} << (q % 64);
+}
+
+char letter(bool xb, bool zb) { return xb ? (zb ? 'Y' : 'X') : (zb ? 'Z' : 'I'); }
+
+// Operands of one compute call, resident on the compute device.
+struct DeviceOperand {
+  DeviceBuffer x, z, c;
+};
+
+DeviceOperand upload(int device, const PauliSum& p) {
+  DeviceOperand d;
+  const std::size_t packed = p.num_terms() * p.words();
+  d.x = abi::upload_vector(device, p.x_words().data(), packed);
+  d.z = abi::upload_vector(device, p.z_words().data(), packed);
+  d.c = abi::upload_vector(device, p.coeffs().data(), p.num_terms());
+  return d;
+}
+
+// Sampled duplicate rate of the first min(T, 512) keys; the reference takes
+// its fused hash-accumulate matmul path when an operand with >= 128 terms has
+// >= 25 % duplicates there (src/multiply.cpp:29-69, :107-109, :179-181).
+bool duplicate_heavy(const PauliSum& p) {
+  if (p.num_terms() < 128) return false;
+  const std::size_t s = std::min<std::size_t>(p.num_terms(), 512);
+  const std::size_t w = p.words();
+  std::vector<std::vector<std::uint64_t>> keys(s);
+  for (std::size_t t = 0; t < s; ++t)
+    for (std::size_t k = 0; k < w; ++k) {
+      keys[t].push_back(p.x_words()[t * w + k]);
+      keys[t].push_back(p.z_words()[t * w + k]);
+    }
+  std::sort(keys.begin(), keys.end());
+  const std::size_t unique = static_cast<std::size_t>(std::unique(keys.begin(), keys.end()) - keys.begin());
+  return 1.0 - static_cast<double>(unique) / static_cast<double>(s) >= 0.25;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ storage
+
+PauliSum::PauliSum(std::size_t num_qubits, std::size_t num_terms)
+    : num_qubits_(num_qubits),
+      words_(guards::word_count(num_qubits)),
+      num_terms_(num_terms),
+      x_(guards::product(num_terms, words_, "x"), 0),
+      z_(guards::product(num_terms, words_, "z"), 0),
+      coeffs_(num_terms, std::complex<double>{0.0, 0.0}) {}
+
+PauliSum::PauliSum(std::size_t num_qubits, std::size_t words, std::size_t num_terms, std::vector<std::uint64_t> x,
+                   std::vector<std::uint64_t> z, std::vector<std::complex<double>> coeffs)
+    : num_qubits_(num_qubits),
+      words_(words),
+      num_terms_(num_terms),
+      x_(std::move(x)),
+      z_(std::move(z)),
+      coeffs_(std::move(coeffs)) {
+  const std::size_t packed = guards::product(num_terms_, words_, "packed");
+  if (x_.size() != packed || z_.size() != packed || coeffs_.size() != num_terms_)
+    throw std::invalid_argument("PauliSum buffer sizes do not match metadata");
+}
+
+PauliSum PauliSum::empty(std::size_t num_qubits) {
+  return PauliSum(num_qubits, guards::word_count(num_qubits), 0, {}, {}, {});
+}
+
+PauliSum PauliSum::from_packed(std::size_t num_qubits, std::vector<std::uint64_t> x, std::vector<std::uint64_t> z,
+                               std::vector<std::complex<double>> coeffs) {
+  const std::size_t words = guards::word_count(num_qubits);
+  const std::size_t T = coeffs.size();
+  if (x.size() != T * words || z.size() != T * words)
+    throw std::invalid_argument("PauliSum buffer sizes do not match metadata");
+  if (words && num_qubits % 64) {
+    const std::uint64_t high = ~((std::uint64_t{1} << (num_qubits % 64)) - 1);
+    for (std::size_t t = 0; t < T; ++t)
+      if ((x[t * words + words - 1] | z[t * words + words - 1]) & high)
+        throw std::invalid_argument("packed Pauli words set bits above num_qubits");
+  }
+  return PauliSum(num_qubits, words, T, std::move(x), std::move(z), std::move(coeffs));
+}
+
+std::size_t PauliSum::num_qubits() const noexcept { return num_qubits_; }
+std::size_t PauliSum::num_terms() const noexcept { return num_terms_; }
+std::size_t PauliSum::words() const noexcept { return words_; }
+const std::vector<std::uint64_t>& PauliSum::x_words() const noexcept { return x_; }
+const std::vector<std::uint64_t>& PauliSum::z_words() const noexcept { return z_; }
+const std::vector<std::complex<double>>& PauliSum::coeffs() const noexcept { return coeffs_; }
+
+// ------------------------------------------------------------------ I/O
+
+PauliSum PauliSum::from_labels(const std::vector<std::string>& labels,
+                               const std::vector<std::complex<double>>& coeffs) {
+  if (labels.empty())
+    throw std::invalid_argument(
+        "PauliSum.from_labels([]) cannot infer num_qubits; use PauliSum.empty(num_qubits)");
+  if (coeffs.size() != labels.size()) throw std::invalid_argument("coefficient count must match label count");
+  const std::size_t n = labels.front().size();
+  const std::size_t words = guards::word_count(n);
+  const std::size_t T = labels.size();
+  std::vector<std::uint64_t> x(guards::product(T, words, "x"), 0), z(guards::product(T, words, "z"), 0);
+  for (std::size_t t = 0; t < T; ++t) {
+    const std::string& label = labels[t];
+    if (label.size() != n) throw std::invalid_argument("all dense labels must have the same length");
+    for (std::size_t i = 0; i < n; ++i) {
+      const char p = label[i];
+      if (!valid_pauli(p)) throw std::invalid_argument("dense labels may contain only I, X, Y, or Z");
+      const std::size_t q = n - 1 - i;  // right-most character is qubit 0
+      if (p == 'X' || p == 'Y') set_bit(x, words, t, q);
+      if (p == 'Z' || p == 'Y') set_bit(z, words, t, q);
+    }
+  }
+  return PauliSum(n, words, T, std::move(x), std::move(z), coeffs);
+}
+
+PauliSum PauliSum::from_sparse_list(const std::vector<SparseTerm>& terms, std::size_t num_qubits) {
+  const std::size_t words = guards::word_count(num_qubits);
+  const std::size_t T = terms.size();
+  std::vector<std::uint64_t> x(guards::product(T, words, "x"), 0), z(guards::product(T, words, "z"), 0);
+  std::vector<std::complex<double>> coeffs;
+  coeffs.reserve(T);
+  for (std::size_t t = 0; t < T; ++t) {
+    const SparseTerm& s = terms[t];
+    if (s.local_pauli_string.size() != s.qubit_indices.size())
+      throw std::invalid_argument("sparse local_pauli_string length must match qubit_indices length");
+    std::unordered_set<std::size_t> seen;
+    for (std::size_t i = 0; i < s.local_pauli_string.size(); ++i) {
+      const char p = s.local_pauli_string[i];
+      if (!valid_pauli(p)) throw std::invalid_argument("sparse local_pauli_string may contain only I, X, Y, or Z");
+      const std::size_t q = s.qubit_indices[i];
+      if (q >= num_qubits) throw std::invalid_argument("sparse qubit index is out of range");
+      if (!seen.insert(q).second) throw std::invalid_argument("sparse term contains a duplicate qubit index");
+      if (p == 'X' || p == 'Y') set_bit(x, words, t, q);
+      if (p == 'Z' || p == 'Y') set_bit(z, words, t, q);
+    }
+    coeffs.push_back(s.coefficient);
+  }
+  return PauliSum(num_qubits, words, T, std::move(x), std::move(z), std::move(coeffs));
+}
+
+std::vector<std::string> PauliSum::to_labels() const {
+  std::vector<std::string> out;
+  out.reserve(num_terms_);
+  for (std::size_t t = 0; t < num_terms_; ++t) {
+    std::string label(num_qubits_, 'I');
+    for (std::size_t q = 0; q < num_qubits_; ++q) {
+      const std::uint64_t bit = std::uint64_t{1} << (q % 64);
+      const std::size_t w = t * words_ + q / 64;
+      label[num_qubits_ - 1 - q] = letter(x_[w] & bit, z_[w] & bit);
+    }
+    out.push_back(std::move(label));
+  }
+  return out;
+}
+
+std::vector<PauliSum::SparseTerm> PauliSum::to_sparse_list() const {
+  std::vector<SparseTerm> out;
+  out.reserve(num_terms_);
+  for (std::size_t t = 0; t < num_terms_; ++t) {
+    SparseTerm s;
+    s.coefficient = coeffs_[t];
+    for (std::size_t q = 0; q < num_qubits_; ++q) {
+      const std::uint64_t bit = std::uint64_t{1} << (q % 64);
+      const std::size_t w = t * words_ + q / 64;
+      const char p = letter(x_[w] & bit, z_[w] & bit);
+      if (p != 'I') {
+        s.local_pauli_string.push_back(p);
+        s.qubit_indices.push_back(q);
+      }
+    }
+    out.push_back(std::move(s));
+  }
+  return out;
+}
+
+// ------------------------------------------------------------------ arithmetic
+
+PauliSum PauliSum::add(const PauliSum& rhs) const {
+  if (num_qubits_ != rhs.num_qubits_) throw std::invalid_argument("PauliSum addition requires the same num_qubits");
+  const std::size_t T = guards::sum(num_terms_, rhs.num_terms_, "terms");
+  std::vector<std::uint64_t> x, z;
+  std::vector<std::complex<double>> c;
+  x.reserve(guards::product(T, words_, "x"));
+  z.reserve(guards::product(T, words_, "z"));
+  c.reserve(T);
+  x.insert(x.end(), x_.begin(), x_.end());
+  x.insert(x.end(), rhs.x_.begin(), rhs.x_.end());
+  z.insert(z.end(), z_.begin(), z_.end());
+  z.insert(z.end(), rhs.z_.begin(), rhs.z_.end());
+  c.insert(c.end(), coeffs_.begin(), coeffs_.end());
+  c.insert(c.end(), rhs.coeffs_.begin(), rhs.coeffs_.end());
+  return PauliSum(num_qubits_, words_, T, std::move(x), std::move(z), std::move(c));
+}
+
+PauliSum PauliSum::scalar_multiply(std::complex<double> scalar) const {
+  std::vector<std::complex<double>> c;
+  c.reserve(coeffs_.size());
+  for (const auto& v : coeffs_) c.push_back(v * scalar);
+  return PauliSum(num_qubits_, words_, num_terms_, x_, z_, std::move(c));
+}
+
+// ------------------------------------------------------------------ device compute
+
+namespace {
+
+PauliSum download_result(std::size_t n, std::size_t words, int device, std::uint64_t* ox, std::uint64_t* oz,
+                         double* oc, std::size_t U) {
+  DeviceBuffer bx = DeviceBuffer::adopt(device, ox, U * words * 8);
+  DeviceBuffer bz = DeviceBuffer::adopt(device, oz, U * words * 8);
+  DeviceBuffer bc = DeviceBuffer::adopt(device, oc, U * 16);
+  if (U == 0) return PauliSum::empty(n);
+  std::vector<std::uint64_t> x(U * words), z(U * words);
+  std::vector<std::complex<double>> c(U);
+  bx.download(x.data(), x.size() * 8);
+  bz.download(z.data(), z.size() * 8);
+  bc.download(c.data(), c.size() * 16);
+  return PauliSum::from_packed(n, std::move(x), std::move(z), std::move(c));
+}
+
+}  // namespace
+
+PauliSum PauliSum::simplify(double atol, double rtol) const {
+  if (atol < 0.0 || rtol < 0.0 || !std::isfinite(atol) || !std::isfinite(rtol))
+    throw std::invalid_argument("simplify tolerances must be non-negative finite values");
+  if (num_terms_ == 0) return PauliSum::empty(num_qubits_);
+  const int dev = abi::compute_device();
+  DeviceOperand d = upload(dev, *this);
+  std::uint64_t *ox = nullptr, *oz = nullptr;
+  double* oc = nullptr;
+  std::size_t U = 0;
+  abi::check(wg_simplify(dev, words_, num_terms_, d.x.as<std::uint64_t>(), d.z.as<std::uint64_t>(),
+                         d.c.as<double>(), atol, rtol, &ox, &oz, &oc, &U, nullptr));
+  return download_result(num_qubits_, words_, dev, ox, oz, oc, U);
+}
+
+PauliSum PauliSum::matmul(const PauliSum& rhs, bool simplify_output, std::size_t max_intermediate_terms) const {
+  if (num_qubits_ != rhs.num_qubits_) throw std::invalid_argument("PauliSum matmul requires the same num_qubits");
+  const std::size_t P = guards::matmul_terms(num_terms_, rhs.num_terms_, max_intermediate_terms);
+  if (P == 0) return PauliSum::empty(num_qubits_);
+  int mode = WG_PRODUCTS_RAW;
+  if (simplify_output) {
+    const bool fused = (words_ == 1 || words_ == 2) && (duplicate_heavy(*this) || duplicate_heavy(rhs));
+    mode = fused ? WG_PRODUCTS_FUSED : WG_PRODUCTS_SIMPLIFY;
+  }
+  const int dev = abi::compute_device();
+  DeviceOperand l = upload(dev, *this), r = upload(dev, rhs);
+  std::uint64_t *ox = nullptr, *oz = nullptr;
+  double* oc = nullptr;
+  std::size_t U = 0;
+  abi::check(wg_pauli_products(dev, words_, l.x.as<std::uint64_t>(), l.z.as<std::uint64_t>(), l.c.as<double>(),
+                               num_terms_, r.x.as<std::uint64_t>(), r.z.as<std::uint64_t>(), r.c.as<double>(),
+                               rhs.num_terms_, mode, 1.0e-12, 0.0, &ox, &oz, &oc, &U, nullptr));
+  if (!simplify_output) {
+    // raw products keep nested-loop order and are returned as-is
+    DeviceBuffer bx = DeviceBuffer::adopt(dev, ox, U * words_ * 8);
+    DeviceBuffer bz = DeviceBuffer::adopt(dev, oz, U * words_ * 8);
+    DeviceBuffer bc = DeviceBuffer::adopt(dev, oc, U * 16);
+    std::vector<std::uint64_t> x(U * words_), z(U * words_);
+    std::vector<std::complex<double>> c(U);
+    bx.download(x.data(), x.size() * 8);
+    bz.download(z.data(), z.size() * 8);
+    bc.download(c.data(), c.size() * 16);
+    return PauliSum(num_qubits_, words_, U, std::move(x), std::move(z), std::move(c));
+  }
+  return download_result(num_qubits_, words_, dev, ox, oz, oc, U);
+}
+
+std::vector<std::uint8_t> PauliSum::commutes_with(const PauliSum& rhs,
+                                                  std::size_t max_commutation_matrix_entries) const {
+  if (num_qubits_ != rhs.num_qubits_)
+    throw std::invalid_argument("PauliSum commutation requires the same num_qubits");
+  const std::size_t entries = guards::commutation_entries(num_terms_, rhs.num_terms_, max_commutation_matrix_entries);
+  std::vector<std::uint8_t> out(entries, 0);
+  if (entries == 0) return out;
+  const int dev = abi::compute_device();
+  DeviceOperand l = upload(dev, *this), r = upload(dev, rhs);
+  const std::size_t pitch = (rhs.num_terms_ + 31) / 32;
+  DeviceBuffer bits(dev, num_terms_ * pitch * 4), flags(dev, entries);
+  abi::check(wg_commutation_bits(dev, words_, l.x.as<std::uint64_t>(), l.z.as<std::uint64_t>(), num_terms_,
+                                 r.x.as<std::uint64_t>(), r.z.as<std::uint64_t>(), rhs.num_terms_,
+                                 bits.as<std::uint32_t>(), pitch, 0, nullptr));
+  abi::check(wg_bits_to_u8(dev, bits.as<std::uint32_t>(), num_terms_, rhs.num_terms_, pitch,
+                           flags.as<std::uint8_t>(), nullptr));
+  flags.download(out.data(), entries);
+  return out;
+}
+
+std::vector<PauliSum> PauliSum::group_commuting(std::string_view mode, std::string_view strategy,
+                                                std::size_t max_terms_for_graph) const {
+  // max_terms_for_graph only chooses between the reference's precomputed-graph
+  // and streaming checks, which give identical groups (src/grouping.cpp:137-193).
+  (void)max_terms_for_graph;
+  if (strategy != "largest_first") throw std::invalid_argument("group_commuting strategy must be 'largest_first'");
+  if (mode != "qwc" && mode != "full") throw std::invalid_argument("group_commuting mode must be 'qwc' or 'full'");
+  if (num_terms_ == 0) return {};
+  const int dev = abi::compute_device();
+  DeviceOperand d = upload(dev, *this);
+  std::vector<std::size_t> order(num_terms_), sizes(num_terms_);
+  std::size_t G = 0;
+  abi::check(wg_group_commuting(dev, words_, num_terms_, d.x.as<std::uint64_t>(), d.z.as<std::uint64_t>(),
+                                mode == "full" ? 1 : 0, order.data(), sizes.data(), &G, nullptr));
+  std::vector<PauliSum> groups;
+  groups.reserve(G);
+  std::size_t p = 0;
+  for (std::size_t g = 0; g < G; ++g) {
+    std::vector<std::uint64_t> x, z;
+    std::vector<std::complex<double>> c;
+    for (std::size_t i = 0; i < sizes[g]; ++i, ++p) {
+      const std::size_t t = order[p];
+      for (std::size_t k = 0; k < words_; ++k) {
+        x.push_back(x_[t * words_ + k]);
+        z.push_back(z_[t * words_ + k]);
+      }
+      c.push_back(coeffs_[t]);
+    }
+    groups.push_back(PauliSum(num_qubits_, words_, sizes[g], std::move(x), std::move(z), std::move(c)));
+  }
+  return groups;
+}
+
+namespace {
+
+template <typename C>
+std::complex<double> expectation_on_device(const PauliSum& op, std::span<const C> psi, int dtype) {
+  guards::statevector_length(op.num_qubits(), psi.size());
+  if (op.num_terms() == 0) return {0.0, 0.0};
+  const int dev = abi::compute_device();
+  DeviceOperand d = upload(dev, op);
+  DeviceBuffer dpsi = abi::upload_vector(dev, psi.data(), psi.size());
+  double out[2] = {0.0, 0.0};
+  abi::check(wg_expectation(dev, op.num_qubits(), op.num_terms(), d.x.as<std::uint64_t>(), d.z.as<std::uint64_t>(),
+                            d.c.as<double>(), dpsi.get(), dtype, out, nullptr));
+  return {out[0], out[1]};
+}
+
+}  // namespace
+
+std::complex<double> PauliSum::expectation_statevector_complex128(std::span<const std::complex<double>> psi) const {
+  return expectation_on_device(*this, psi, WG_DTYPE_C128);
+}
+
+std::complex<double> PauliSum::expectation_statevector_complex64(std::span<const std::complex<float>> psi) const {
+  return expectation_on_device(*this, psi, WG_DTYPE_C64);
+}
+
+std::complex<double> PauliSum::expectation_z_counts(const std::vector<std::string>& bitstrings,
+                                                    const std::vector<double>& counts) const {
+  // Validation order and messages of src/expectation.cpp:157-230.
+  if (bitstrings.size() != counts.size())
+    throw std::invalid_argument("Z-count bitstring and count arrays must have the same length");
+  for (std::uint64_t w : x_)
+    if (w != 0) throw std::invalid_argument("expectation_z_counts requires diagonal Pauli terms");
+  double total = 0.0;
+  for (double v : counts) {
+    if (v < 0.0) throw std::invalid_argument("Z-count values must be non-negative");
+    if (!std::isfinite(v)) throw std::invalid_argument("Z-count values must be finite");
+    total += v;
+  }
+  if (total <= 0.0) throw std::invalid_argument("Z-count total count must be positive");
+  const std::size_t rows = bitstrings.size();
+  std::vector<std::uint64_t> packed(guards::product(rows, words_, "counts"), 0);
+  for (std::size_t r = 0; r < rows; ++r) {
+    const std::string& b = bitstrings[r];
+    if (b.size() != num_qubits_) throw std::invalid_argument("Z-count bitstring length must equal num_qubits");
+    for (std::size_t i = 0; i < b.size(); ++i) {
+      if (b[i] != '0' && b[i] != '1') throw std::invalid_argument("Z-count bitstrings may contain only 0 or 1");
+      if (b[i] == '1') {
+        const std::size_t q = num_qubits_ - 1 - i;
+        packed[r * words_ + q / 64] |= std::uint64_t{1} << (q % 64);
+      }
+    }
+  }
+  if (num_terms_ == 0) return {0.0, 0.0};
+  const int dev = abi::compute_device();
+  DeviceOperand d = upload(dev, *this);
+  DeviceBuffer dp = abi::upload_vector(dev, packed.data(), packed.size());
+  DeviceBuffer dc = abi::upload_vector(dev, counts.data(), counts.size());
+  double out[2] = {0.0, 0.0};
+  abi::check(wg_expectation_z_counts(dev, words_, num_terms_, d.x.as<std::uint64_t>(), d.z.as<std::uint64_t>(),
+                                     d.c.as<double>(), rows, dp.as<std::uint64_t>(), dc.as<double>(), out, nullptr));
+  return {out[0], out[1]};
+}
+
+std::size_t PauliSum::checked_matmul_intermediate_terms_for_testing(std::size_t lhs_terms, std::size_t rhs_terms,
+                                                                     std::size_t max_intermediate_terms) {
+  return guards::matmul_terms(lhs_terms, rhs_terms, max_intermediate_terms);
+}
+
+std::size_t PauliSum::checked_commutation_matrix_entries_for_testing(std::size_t lhs_terms, std::size_t rhs_terms,
+                                                                      std::size_t max_commutation_matrix_entries) {
+  return guards::commutation_entries(lhs_terms, rhs_terms, max_commutation_matrix_entries);
+}
+
+}  // namespace wolfgang

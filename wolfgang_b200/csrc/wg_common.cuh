@@ -1,0 +1,301 @@
+// wg_common.cuh -- shared host/device plumbing for the sm_100a packed-Pauli kernels.
+//
+// Host side: thread-local error text, status codes, checked CUDA calls, and the
+// device-property cache used to size grids in multiples of the SM count.
+// Device side: exact-rounding FP64 complex helpers and key utilities.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "wg_pauli.h"
+
+namespace wg {
+
+// ---------------------------------------------------------------- host errors
+
+void set_error(const std::string& msg);
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void throw_invalid(const std::string& m) { throw Error(WG_ERR_INVALID, m); }
+
+inline void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  (void)cudaGetLastError();
+  const int code = (e == cudaErrorMemoryAllocation) ? WG_ERR_OOM : WG_ERR_CUDA;
+  throw Error(code, std::string("CUDA ") + what + " failed: " + cudaGetErrorString(e));
+}
+
+// Optional per-kernel timing (wg_profile_enable): a ProfRange placed before a
+// launch records CUDA events on the launch stream around it; durations are
+// summed per kernel name by wg_profile_report.
+bool profiling();
+void prof_record(const char* name, cudaStream_t s, bool begin);
+struct ProfRange {
+  const char* name;
+  cudaStream_t s;
+  bool on;
+  ProfRange(const char* n, cudaStream_t st) : name(n), s(st), on(profiling()) {
+    if (on) prof_record(name, s, true);
+  }
+  ~ProfRange() {
+    if (on) prof_record(name, s, false);
+  }
+};
+
+// Launch wrapped in a timing range named `name` on `stream`.
+#define WG_TIMED(name, stream, ...)       \
+  do {                                    \
+    ::wg::ProfRange wg_prof_(name, stream); \
+    __VA_ARGS__;                          \
+  } while (0)
+
+// Every kernel launch site calls check_launch, which also counts launches
+// (wg_kernel_launches reports the total).
+void count_launch();
+inline void check_launch(const char* what) {
+  count_launch();
+  check_cuda(cudaGetLastError(), what);
+}
+
+// Runs f(), mapping exceptions onto the C-ABI status convention.
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return WG_OK;
+  } catch (const Error& e) {
+    set_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return WG_ERR_OOM;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return WG_ERR_INVALID;
+  }
+}
+
+// Per-device properties, cached after the first query.
+struct DeviceProps {
+  int sm_count = 0;
+  int max_smem_optin = 0;
+  size_t l2_bytes = 0;
+};
+const DeviceProps& device_props(int device);
+int current_device();
+
+// Grid size for a grid-stride kernel: a whole number of waves of `per_sm`
+// resident CTAs on every SM, never more blocks than work items need.
+inline unsigned grid_for(size_t items, unsigned block_items, int device, int per_sm) {
+  const size_t need = (items + block_items - 1) / block_items;
+  const size_t wave = static_cast<size_t>(device_props(device).sm_count) * per_sm;
+  size_t g = need < wave ? need : wave;
+  if (g == 0) g = 1;
+  return static_cast<unsigned>(g);
+}
+
+// Stream-ordered scratch from the device's default memory pool (cached by the
+// pool between calls).  Freed on the same stream when the holder dies.
+class Scratch {
+ public:
+  Scratch() = default;
+  Scratch(size_t bytes, cudaStream_t s) { reset(bytes, s); }
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+  Scratch(Scratch&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) { o.p_ = nullptr; }
+  Scratch& operator=(Scratch&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_;
+      n_ = o.n_;
+      s_ = o.s_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  ~Scratch() { release(); }
+  void reset(size_t bytes, cudaStream_t s);
+  void release() noexcept;
+  void* get() const { return p_; }
+  template <typename T>
+  T* as() const { return static_cast<T*>(p_); }
+  size_t size() const { return n_; }
+  // Stream on which the buffer is released (for buffers that outlive the
+  // stream they were allocated on).
+  void rebind(cudaStream_t s) { s_ = s; }
+  // Hands ownership to the caller (the result buffers of an entry point).
+  void* detach() {
+    void* p = p_;
+    p_ = nullptr;
+    n_ = 0;
+    return p;
+  }
+
+ private:
+  void* p_ = nullptr;
+  size_t n_ = 0;
+  cudaStream_t s_ = nullptr;
+};
+
+// RAII device switch for entry points that take an explicit ordinal.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int device) {
+    int count = 0;
+    const cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+      (void)cudaGetLastError();
+      throw Error(WG_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    if (device < 0 || device >= count) throw_invalid("CUDA device ordinal is out of range");
+    check_cuda(cudaGetDevice(&prev), "get current device");
+    if (prev != device) check_cuda(cudaSetDevice(device), "set device");
+    (void)device_props(device);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) (void)cudaSetDevice(prev);
+  }
+};
+
+void* pool_alloc(size_t bytes, cudaStream_t s);
+void pool_free(void* p, cudaStream_t s) noexcept;
+
+// Stable LSD radix sort of n items by K structure-of-arrays key words (word 0
+// most significant) carrying a 32-bit item index (wg_simplify.cu).
+void radix_sort_keys(int device, size_t n, int K, Scratch& keys, Scratch& idx, cudaStream_t s);
+
+inline size_t checked_mul(size_t a, size_t b, const char* what) {
+  if (a != 0 && b > SIZE_MAX / a) throw_invalid(std::string(what) + " size overflows size_t");
+  return a * b;
+}
+
+}  // namespace wg
+
+// ============================================================== device helpers
+namespace wgd {
+
+struct c128 {
+  double re, im;
+};
+
+// IEEE operations with explicit round-to-nearest and no contraction, so each
+// product or sum rounds once, as in the reference's g++ -O2 build (x86-64
+// baseline code generation has no FMA).
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+__device__ __forceinline__ c128 cadd(c128 a, c128 b) { return {add(a.re, b.re), add(a.im, b.im)}; }
+
+// std::complex<double> multiplication as g++ evaluates it without
+// -ffast-math / -fcx-limited-range: (ac - bd, ad + bc), and when both parts are
+// NaN the recovery procedure of ISO C Annex G.5.1 (the algorithm libgcc's
+// __muldc3 implements) to recover infinities.
+__device__ __forceinline__ c128 cmul(c128 z, c128 w) {
+  double a = z.re, b = z.im, c = w.re, d = w.im;
+  const double ac = mul(a, c), bd = mul(b, d), ad = mul(a, d), bc = mul(b, c);
+  double x = sub(ac, bd), y = add(ad, bc);
+  if (isnan(x) && isnan(y)) {
+    bool recalc = false;
+    if (isinf(a) || isinf(b)) {
+      a = copysign(isinf(a) ? 1.0 : 0.0, a);
+      b = copysign(isinf(b) ? 1.0 : 0.0, b);
+      if (isnan(c)) c = copysign(0.0, c);
+      if (isnan(d)) d = copysign(0.0, d);
+      recalc = true;
+    }
+    if (isinf(c) || isinf(d)) {
+      c = copysign(isinf(c) ? 1.0 : 0.0, c);
+      d = copysign(isinf(d) ? 1.0 : 0.0, d);
+      if (isnan(a)) a = copysign(0.0, a);
+      if (isnan(b)) b = copysign(0.0, b);
+      recalc = true;
+    }
+    if (!recalc && (isinf(ac) || isinf(bd) || isinf(ad) || isinf(bc))) {
+      if (isnan(a)) a = copysign(0.0, a);
+      if (isnan(b)) b = copysign(0.0, b);
+      if (isnan(c)) c = copysign(0.0, c);
+      if (isnan(d)) d = copysign(0.0, d);
+      recalc = true;
+    }
+    if (recalc) {
+      x = mul(__longlong_as_double(0x7ff0000000000000LL), sub(mul(a, c), mul(b, d)));
+      y = mul(__longlong_as_double(0x7ff0000000000000LL), add(mul(a, d), mul(b, c)));
+    }
+  }
+  return {x, y};
+}
+
+// Multiplication by i^e (exact sign swaps).
+__device__ __forceinline__ c128 rotate(c128 v, unsigned e) {
+  switch (e & 3U) {
+    case 0: return v;
+    case 1: return {-v.im, v.re};
+    case 2: return {-v.re, -v.im};
+    default: return {v.im, -v.re};
+  }
+}
+
+// |z| with the rounding of glibc's hypot, which std::abs(std::complex<double>)
+// calls in the reference.  The method is the corrected square root of
+// C. F. Borges, "An Improved Algorithm for hypot(a,b)" (arXiv:1904.09481), in
+// its variant without fused multiply-add, with power-of-two rescaling outside
+// [2^-500, 2^500] and the large-ratio shortcut; checked bit-for-bit against the
+// host libm across the full exponent range by the test suite.
+__device__ __forceinline__ double borges_kernel(double ax, double ay) {
+  double h = __dsqrt_rn(add(mul(ax, ax), mul(ay, ay)));
+  double t1, t2;
+  if (h <= mul(2.0, ay)) {
+    const double delta = sub(h, ay);
+    t1 = mul(ax, sub(mul(2.0, delta), ax));
+    t2 = mul(sub(delta, mul(2.0, sub(ax, ay))), delta);
+  } else {
+    const double delta = sub(h, ax);
+    t1 = mul(mul(2.0, delta), sub(ax, mul(2.0, ay)));
+    t2 = add(mul(sub(mul(4.0, delta), ay), ay), mul(delta, delta));
+  }
+  return sub(h, __ddiv_rn(add(t1, t2), mul(2.0, h)));
+}
+
+__device__ __forceinline__ double hypot_ref(double x, double y) {
+  if (isinf(x) || isinf(y)) return __longlong_as_double(0x7ff0000000000000LL);
+  if (isnan(x) || isnan(y)) return __longlong_as_double(0x7ff8000000000000LL);
+  double ax = fabs(x), ay = fabs(y);
+  if (ax < ay) {
+    const double t = ax;
+    ax = ay;
+    ay = t;
+  }
+  if (ay == 0.0) return ax;
+  if (ax > mul(ay, 0x1p54)) return add(ax, ay);
+  if (ax > 0x1p500) return mul(borges_kernel(mul(ax, 0x1p-600), mul(ay, 0x1p-600)), 0x1p600);
+  if (ay < 0x1p-500) return mul(borges_kernel(mul(ax, 0x1p600), mul(ay, 0x1p600)), 0x1p-600);
+  return borges_kernel(ax, ay);
+}
+
+__device__ __forceinline__ unsigned popc64(uint64_t v) { return __popcll(v); }
+
+// Strict canonical comparison of two keys held as 2*W words in significance
+// order (x0, z0, x1, z1, ...).
+template <int W>
+__device__ __forceinline__ bool key_less(const uint64_t (&a)[2 * W], const uint64_t (&b)[2 * W]) {
+#pragma unroll
+  for (int i = 0; i < 2 * W; ++i)
+    if (a[i] != b[i]) return a[i] < b[i];
+  return false;
+}
+
+}  // namespace wgd

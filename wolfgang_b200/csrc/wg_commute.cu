@@ -1,0 +1,480 @@
+// wg_commute.cu -- bit-packed all-pairs commutation matrix and its consumers.
+//
+// Semantics (reference src/detail/commutation.hpp:10-46, src/commute.cpp:27-93):
+// terms l and r commute iff parity(sum_w popc((lx_w & rz_w) ^ (lz_w & rx_w))) == 0.
+// Because parity is additive over XOR, all words fold into one 64-bit value
+// before a single population count.
+//
+// Output: bits[row*pitch + c/32] bit (c%32) = 1 iff (row, c) commute.  The
+// reference writes one byte per entry (src/cuda/commutation_cuda.cu:123-151);
+// the bit matrix is 8x smaller, which is what bounds the kernel at large sizes.
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "wg_common.cuh"
+
+namespace {
+
+constexpr int kColsPerLane = 8;                    // rhs columns held in registers per lane
+constexpr int kWarpCols = 32 * kColsPerLane;       // 256 columns = 8 output words per warp
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRowsPerWarpIter = 64;               // rows a warp sweeps per column tile
+
+// ---------------------------------------------------------------------------
+// algo 1: popcount / LOP3 with warp-ballot packing.
+// CTA = one 256-column tile x (kWarps * kRowsPerWarpIter) rows.  Every lane
+// keeps the masks of its 8 columns in registers; each row's masks are a
+// broadcast load; the 8 ballots of a row give 8 consecutive output words,
+// stored by lanes 0..7 as one 32-byte sector.
+template <int W>
+__global__ void __launch_bounds__(kThreads) commute_ballot_kernel(
+    const uint64_t* __restrict__ lx, const uint64_t* __restrict__ lz, size_t n_l,
+    const uint64_t* __restrict__ rx, const uint64_t* __restrict__ rz, size_t n_r,
+    uint32_t* __restrict__ bits, size_t pitch) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const size_t col_tile = blockIdx.x;
+  const size_t col0 = col_tile * kWarpCols;
+  const size_t words_needed = (n_r + 31) / 32;
+
+  uint64_t cx[kColsPerLane][W], cz[kColsPerLane][W];
+  uint32_t valid = 0;  // bit k: column k of this lane exists
+#pragma unroll
+  for (int k = 0; k < kColsPerLane; ++k) {
+    const size_t c = col0 + 32 * k + lane;
+    const bool ok = c < n_r;
+    valid |= ok ? (1u << k) : 0u;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      cx[k][w] = ok ? __ldg(rx + c * W + w) : 0;
+      cz[k][w] = ok ? __ldg(rz + c * W + w) : 0;
+    }
+  }
+  // Word k of this tile holds columns col0 + 32k + lane; mask off absent ones.
+  uint32_t word_valid[kColsPerLane];
+#pragma unroll
+  for (int k = 0; k < kColsPerLane; ++k) word_valid[k] = __ballot_sync(0xffffffffu, (valid >> k) & 1u);
+
+  const size_t row_begin = static_cast<size_t>(blockIdx.y) * (kWarps * kRowsPerWarpIter) + warp;
+  const size_t row_end = min(n_l, static_cast<size_t>(blockIdx.y + 1) * (kWarps * kRowsPerWarpIter));
+  for (size_t row = row_begin; row < row_end; row += kWarps) {
+    uint64_t ax[W], az[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      ax[w] = __ldg(lx + row * W + w);
+      az[w] = __ldg(lz + row * W + w);
+    }
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < kColsPerLane; ++k) {
+      uint64_t acc = 0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) acc ^= (ax[w] & cz[k][w]) ^ (az[w] & cx[k][w]);
+      const uint32_t folded = static_cast<uint32_t>(acc) ^ static_cast<uint32_t>(acc >> 32);
+      const bool commute = (__popc(folded) & 1u) == 0;
+      const uint32_t word = __ballot_sync(0xffffffffu, commute) & word_valid[k];
+      if (lane == k) mine = word;
+    }
+    const size_t wi = col_tile * kColsPerLane + lane;
+    if (lane < kColsPerLane && wi < words_needed) bits[row * pitch + wi] = mine;
+  }
+}
+
+// Generic word count (W > 4): masks read per pair from global/L1.
+__global__ void __launch_bounds__(kThreads) commute_generic_kernel(
+    const uint64_t* __restrict__ lx, const uint64_t* __restrict__ lz, size_t n_l,
+    const uint64_t* __restrict__ rx, const uint64_t* __restrict__ rz, size_t n_r, size_t W,
+    uint32_t* __restrict__ bits, size_t pitch) {
+  const int lane = threadIdx.x & 31;
+  const size_t words_needed = (n_r + 31) / 32;
+  const size_t total = n_l * words_needed;
+  const size_t warp_global = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = (static_cast<size_t>(gridDim.x) * blockDim.x) >> 5;
+  for (size_t item = warp_global; item < total; item += nwarps) {
+    const size_t row = item / words_needed;
+    const size_t wi = item - row * words_needed;
+    const size_t c = wi * 32 + lane;
+    bool commute = false;
+    if (c < n_r) {
+      uint64_t acc = 0;
+      for (size_t w = 0; w < W; ++w)
+        acc ^= (lx[row * W + w] & rz[c * W + w]) ^ (lz[row * W + w] & rx[c * W + w]);
+      commute = (__popcll(acc) & 1u) == 0;
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, commute);
+    if (lane == 0) bits[row * pitch + wi] = word;
+  }
+}
+
+// n_qubits == 0: every pair commutes.
+__global__ void fill_ones_kernel(uint32_t* bits, size_t rows, size_t cols, size_t pitch) {
+  const size_t words_needed = (cols + 31) / 32;
+  const size_t total = rows * words_needed;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t row = i / words_needed;
+    const size_t wi = i - row * words_needed;
+    const size_t rem = cols - wi * 32;
+    bits[row * pitch + wi] = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// algo 2: bit-plane XOR.  For a block of 32*kPlaneWords rhs columns, plane
+// (q, X|Z) is the bit-vector over the block of the rhs x/z bits on qubit q.
+// Row l's output word j is the complement of XOR over q in supp(l) of
+// (lx_q ? Zplane_q[j] : 0) ^ (lz_q ? Xplane_q[j] : 0).  Per output word that
+// is ~weight(l) shared-memory reads instead of 32 * (4W LOP3 + POPC), so for
+// sparse terms the kernel is bound by the output write.
+constexpr int kPlaneWords = 32;  // output words per row per CTA (1024 columns)
+
+template <int W>
+__global__ void __launch_bounds__(kThreads) commute_plane_kernel(
+    const uint64_t* __restrict__ lx, const uint64_t* __restrict__ lz, size_t n_l,
+    const uint64_t* __restrict__ rx, const uint64_t* __restrict__ rz, size_t n_r,
+    uint32_t* __restrict__ bits, size_t pitch, size_t rows_per_cta) {
+  // planes[(q*2 + 0)*32 + j] = X bits of rhs block word j on qubit q; +1 = Z bits.
+  extern __shared__ uint32_t planes[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const size_t col0 = static_cast<size_t>(blockIdx.x) * (32 * kPlaneWords);
+  const size_t words_needed = (n_r + 31) / 32;
+  // Build: warp handles block words j = warp, warp+8, ...; lane t loads column
+  // col0 + 32j + t once, then one ballot per (qubit, x|z) gives a plane word.
+  for (int j = warp; j < kPlaneWords; j += kWarps) {
+    const size_t c = col0 + 32 * static_cast<size_t>(j) + lane;
+    const bool ok = c < n_r;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const uint64_t vx = ok ? __ldg(rx + c * W + w) : 0;
+      const uint64_t vz = ok ? __ldg(rz + c * W + w) : 0;
+#pragma unroll 8
+      for (int b = 0; b < 64; ++b) {
+        const uint32_t px = __ballot_sync(0xffffffffu, (vx >> b) & 1u);
+        const uint32_t pz = __ballot_sync(0xffffffffu, (vz >> b) & 1u);
+        if (lane == (b & 31)) {
+          const int q = w * 64 + b;
+          planes[(q * 2 + 0) * kPlaneWords + j] = px;
+          planes[(q * 2 + 1) * kPlaneWords + j] = pz;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  uint32_t valid = 0xffffffffu;
+  {
+    const size_t c_first = col0 + 32 * static_cast<size_t>(lane);
+    if (c_first >= n_r) valid = 0;
+    else if (n_r - c_first < 32) valid = (1u << (n_r - c_first)) - 1u;
+  }
+  const size_t wi = static_cast<size_t>(blockIdx.x) * kPlaneWords + lane;
+  const size_t row0 = static_cast<size_t>(blockIdx.y) * rows_per_cta;
+  const size_t row1 = min(n_l, row0 + rows_per_cta);
+  for (size_t row = row0 + warp; row < row1; row += kWarps) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const uint64_t ax = __ldg(lx + row * W + w);
+      const uint64_t az = __ldg(lz + row * W + w);
+      uint64_t sup = ax | az;
+      while (sup) {
+        const int b = __ffsll(static_cast<long long>(sup)) - 1;
+        sup &= sup - 1;
+        const int q = w * 64 + b;
+        const uint32_t mx = 0u - static_cast<uint32_t>((ax >> b) & 1u);  // lhs X on q -> rhs Z plane
+        const uint32_t mz = 0u - static_cast<uint32_t>((az >> b) & 1u);  // lhs Z on q -> rhs X plane
+        acc ^= (planes[(q * 2 + 1) * kPlaneWords + lane] & mx) ^ (planes[(q * 2 + 0) * kPlaneWords + lane] & mz);
+      }
+    }
+    if (wi < words_needed) bits[row * pitch + wi] = ~acc & valid;
+  }
+}
+
+template <int W>
+void launch_ballot(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
+                   const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, cudaStream_t s) {
+  const size_t col_tiles = (n_r + kWarpCols - 1) / kWarpCols;
+  const size_t row_chunks = (n_l + kWarps * kRowsPerWarpIter - 1) / (kWarps * kRowsPerWarpIter);
+  if (row_chunks > 65535) {
+    // Split the launch along rows to respect gridDim.y.
+    const size_t rows_per_launch = 65535ull * kWarps * kRowsPerWarpIter;
+    for (size_t r0 = 0; r0 < n_l; r0 += rows_per_launch) {
+      const size_t nrows = min(rows_per_launch, n_l - r0);
+      launch_ballot<W>(lx + r0 * W, lz + r0 * W, nrows, rx, rz, n_r, bits + r0 * pitch, pitch, s);
+    }
+    return;
+  }
+  dim3 grid(static_cast<unsigned>(col_tiles), static_cast<unsigned>(row_chunks));
+  WG_TIMED("commute_ballot_kernel", s,
+    commute_ballot_kernel<W><<<grid, kThreads, 0, s>>>(lx, lz, n_l, rx, rz, n_r, bits, pitch));
+  wg::check_launch("launch commutation (ballot)");
+}
+
+template <int W>
+void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
+                  const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, int device,
+                  cudaStream_t s) {
+  const size_t smem = static_cast<size_t>(64 * W) * 2 * kPlaneWords * sizeof(uint32_t);
+  static bool configured[64] = {};
+  if (!configured[device & 63]) {
+    wg::check_cuda(cudaFuncSetAttribute(commute_plane_kernel<W>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "configure bit-plane commutation");
+    configured[device & 63] = true;
+  }
+  const size_t col_blocks = (n_r + 32 * kPlaneWords - 1) / (32 * kPlaneWords);
+  // Enough row chunks to fill the machine; rows per CTA amortise plane building.
+  const size_t sms = wg::device_props(device).sm_count;
+  size_t rows_per_cta = 2048;
+  while (rows_per_cta > 64 && col_blocks * ((n_l + rows_per_cta - 1) / rows_per_cta) < 4 * sms)
+    rows_per_cta /= 2;
+  size_t row_chunks = (n_l + rows_per_cta - 1) / rows_per_cta;
+  while (row_chunks > 65535) {
+    rows_per_cta *= 2;
+    row_chunks = (n_l + rows_per_cta - 1) / rows_per_cta;
+  }
+  dim3 grid(static_cast<unsigned>(col_blocks), static_cast<unsigned>(row_chunks));
+  WG_TIMED("commute_plane_kernel", s,
+    commute_plane_kernel<W><<<grid, kThreads, smem, s>>>(lx, lz, n_l, rx, rz, n_r, bits, pitch, rows_per_cta));
+  wg::check_launch("launch commutation (bit-plane)");
+}
+
+// Autotuned choice between the two algorithms.  Cost model per output word:
+//   ballot: 32 pairs * (4W LOP3 + 1 POPC)  (compute; ~independent of weight)
+//   plane : mean lhs weight smem XORs (+ plane build per CTA)
+// The mean weight is estimated from a sample of lhs rows on the host side of
+// the launch (read back from the device: 256 rows at most).
+int choose_algo(size_t W, const uint64_t* lx, const uint64_t* lz, size_t n_l, size_t n_r,
+                cudaStream_t s) {
+  if (W > 4 || n_r < 512 || n_l < 64) return 1;
+  const size_t sample = n_l < 256 ? n_l : 256;
+  std::vector<uint64_t> hx(sample * W), hz(sample * W);
+  wg::check_cuda(cudaMemcpyAsync(hx.data(), lx, hx.size() * 8, cudaMemcpyDeviceToHost, s), "sample lhs");
+  wg::check_cuda(cudaMemcpyAsync(hz.data(), lz, hz.size() * 8, cudaMemcpyDeviceToHost, s), "sample lhs");
+  wg::check_cuda(cudaStreamSynchronize(s), "sample lhs");
+  size_t weight = 0;
+  for (size_t i = 0; i < hx.size(); ++i) weight += __builtin_popcountll(hx[i] | hz[i]);
+  const double mean_w = static_cast<double>(weight) / static_cast<double>(sample);
+  const double ballot_cost = 32.0 * (4.0 * W + 2.0);  // instructions per output word
+  const double plane_cost = 8.0 * mean_w + 16.0;        // per output word
+  return plane_cost < ballot_cost ? 2 : 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                        size_t n_lhs, const uint64_t* rhs_x, const uint64_t* rhs_z, size_t n_rhs,
+                        uint32_t* bits, size_t pitch_words, int algo, wg_stream_t stream) {
+  return wg::guarded([&] {
+    if (pitch_words < (n_rhs + 31) / 32) wg::throw_invalid("commutation bit matrix pitch is too small");
+    if (algo < 0 || algo > 2) wg::throw_invalid("commutation algo must be 0, 1 or 2");
+    if (n_lhs == 0 || n_rhs == 0) return;
+    wg::DeviceGuard g(device);
+    (void)wg::checked_mul(n_lhs, pitch_words, "commutation bit matrix");
+    cudaStream_t s = stream;
+    if (words == 0) {
+      fill_ones_kernel<<<wg::grid_for(n_lhs * pitch_words, 256, device, 8), 256, 0, s>>>(bits, n_lhs, n_rhs,
+                                                                                          pitch_words);
+      wg::check_launch("launch commutation fill");
+      return;
+    }
+    if (algo == 0) algo = choose_algo(words, lhs_x, lhs_z, n_lhs, n_rhs, s);
+    if (algo == 2 && words <= 4) {
+      switch (words) {
+        case 1: launch_plane<1>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
+        case 2: launch_plane<2>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
+        case 3: launch_plane<3>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
+        case 4: launch_plane<4>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
+      }
+    }
+    switch (words) {
+      case 1: launch_ballot<1>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
+      case 2: launch_ballot<2>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
+      case 3: launch_ballot<3>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
+      case 4: launch_ballot<4>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
+      default: {
+        const size_t items = n_lhs * ((n_rhs + 31) / 32);
+        WG_TIMED("commute_generic_kernel", s,
+          commute_generic_kernel<<<wg::grid_for(items * 32, 256, device, 8), 256, 0, s>>>(
+              lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, words, bits, pitch_words));
+        wg::check_launch("launch commutation (generic)");
+      }
+    }
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// One thread per output byte group of 4 (uint32 store of four 0/1 flags).
+__global__ void bits_to_u8_kernel(const uint32_t* __restrict__ bits, size_t rows, size_t cols,
+                                  size_t pitch, uint8_t* __restrict__ out) {
+  const size_t quads = (cols + 3) / 4;
+  const size_t total = rows * quads;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t row = i / quads;
+    const size_t q = i - row * quads;
+    const size_t c0 = q * 4;
+    const uint32_t word = bits[row * pitch + c0 / 32];
+    const uint32_t nib = (word >> (c0 % 32)) & 0xFu;
+    const size_t base = row * cols + c0;
+    if (c0 + 4 <= cols && ((reinterpret_cast<uintptr_t>(out) + base) & 3) == 0) {
+      const uint32_t v = (nib & 1u) | ((nib >> 1) & 1u) << 8 | ((nib >> 2) & 1u) << 16 | ((nib >> 3) & 1u) << 24;
+      *reinterpret_cast<uint32_t*>(out + base) = v;
+    } else {
+      for (size_t k = 0; k < 4 && c0 + k < cols; ++k) out[base + k] = (nib >> k) & 1u;
+    }
+  }
+}
+
+// Row counts: one warp per row.
+__global__ void bits_row_count_kernel(const uint32_t* __restrict__ bits, size_t rows, size_t cols,
+                                      size_t pitch, uint64_t* __restrict__ row_counts,
+                                      unsigned long long* __restrict__ total) {
+  const int lane = threadIdx.x & 31;
+  const size_t words = (cols + 31) / 32;
+  const size_t warp = (blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5;
+  const size_t nwarps = (static_cast<size_t>(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long mine = 0;
+  for (size_t row = warp; row < rows; row += nwarps) {
+    unsigned long long cnt = 0;
+    for (size_t j = lane; j < words; j += 32) cnt += __popc(bits[row * pitch + j]);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && row_counts) row_counts[row] = cnt;
+    mine += cnt;
+  }
+  if (lane == 0 && total) atomicAdd(total, mine);
+}
+
+// Column counts: thread per column, rows in chunks (blockIdx.y), atomics per chunk.
+__global__ void bits_col_count_kernel(const uint32_t* __restrict__ bits, size_t rows, size_t cols,
+                                      size_t pitch, size_t rows_per_chunk,
+                                      unsigned long long* __restrict__ col_counts) {
+  const size_t c = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+  if (c >= cols) return;
+  const size_t r0 = blockIdx.y * rows_per_chunk;
+  const size_t r1 = min(rows, r0 + rows_per_chunk);
+  unsigned long long cnt = 0;
+  for (size_t r = r0; r < r1; ++r) cnt += (bits[r * pitch + c / 32] >> (c % 32)) & 1u;
+  atomicAdd(col_counts + c, cnt);
+}
+
+__global__ void u8_row_count_kernel(const uint8_t* __restrict__ f, size_t rows, size_t cols,
+                                    uint64_t* __restrict__ row_counts, unsigned long long* __restrict__ total) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5;
+  const size_t nwarps = (static_cast<size_t>(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long mine = 0;
+  for (size_t row = warp; row < rows; row += nwarps) {
+    unsigned long long cnt = 0;
+    for (size_t j = lane; j < cols; j += 32) cnt += f[row * cols + j] != 0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && row_counts) row_counts[row] = cnt;
+    mine += cnt;
+  }
+  if (lane == 0 && total) atomicAdd(total, mine);
+}
+
+__global__ void u8_col_count_kernel(const uint8_t* __restrict__ f, size_t rows, size_t cols,
+                                    size_t rows_per_chunk, unsigned long long* __restrict__ col_counts) {
+  const size_t c = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+  if (c >= cols) return;
+  const size_t r0 = blockIdx.y * rows_per_chunk;
+  const size_t r1 = min(rows, r0 + rows_per_chunk);
+  unsigned long long cnt = 0;
+  for (size_t r = r0; r < r1; ++r) cnt += f[r * cols + c] != 0;
+  atomicAdd(col_counts + c, cnt);
+}
+
+template <typename RowK, typename ColK>
+void run_counts(int device, size_t rows, size_t cols, uint64_t* row_counts, uint64_t* col_counts,
+                uint64_t* total, cudaStream_t s, RowK row_launch, ColK col_launch) {
+  wg::Scratch tot(sizeof(unsigned long long), s);
+  wg::check_cuda(cudaMemsetAsync(tot.get(), 0, sizeof(unsigned long long), s), "clear count");
+  if (rows > 0 && cols > 0) {
+    row_launch(tot.as<unsigned long long>());
+    if (col_counts) {
+      wg::check_cuda(cudaMemsetAsync(col_counts, 0, cols * sizeof(uint64_t), s), "clear column counts");
+      col_launch(reinterpret_cast<unsigned long long*>(col_counts));
+    }
+  } else {
+    if (row_counts && rows) wg::check_cuda(cudaMemsetAsync(row_counts, 0, rows * 8, s), "clear row counts");
+    if (col_counts && cols) wg::check_cuda(cudaMemsetAsync(col_counts, 0, cols * 8, s), "clear column counts");
+  }
+  if (total) {
+    unsigned long long h = 0;
+    wg::check_cuda(cudaMemcpyAsync(&h, tot.get(), sizeof(h), cudaMemcpyDeviceToHost, s), "read count");
+    wg::check_cuda(cudaStreamSynchronize(s), "read count");
+    *total = h;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int wg_bits_to_u8(int device, const uint32_t* bits, size_t rows, size_t cols, size_t pitch_words,
+                  uint8_t* out, wg_stream_t stream) {
+  return wg::guarded([&] {
+    if (rows == 0 || cols == 0) return;
+    wg::DeviceGuard g(device);
+    const size_t total = rows * ((cols + 3) / 4);
+    WG_TIMED("bits_to_u8_kernel", stream,
+      bits_to_u8_kernel<<<wg::grid_for(total, 256, device, 8), 256, 0, stream>>>(bits, rows, cols, pitch_words, out));
+    wg::check_launch("launch bits to u8");
+  });
+}
+
+int wg_bits_count(int device, const uint32_t* bits, size_t rows, size_t cols, size_t pitch_words,
+                  uint64_t* row_counts, uint64_t* col_counts, uint64_t* total, wg_stream_t stream) {
+  return wg::guarded([&] {
+    wg::DeviceGuard g(device);
+    cudaStream_t s = stream;
+    run_counts(
+        device, rows, cols, row_counts, col_counts, total, s,
+        [&](unsigned long long* tot) {
+          bits_row_count_kernel<<<wg::grid_for(rows * 32, 256, device, 8), 256, 0, s>>>(bits, rows, cols, pitch_words,
+                                                                                       row_counts, tot);
+          wg::check_launch("launch row counts");
+        },
+        [&](unsigned long long* cc) {
+          const size_t chunk = 4096;
+          dim3 grid(static_cast<unsigned>((cols + 255) / 256), static_cast<unsigned>((rows + chunk - 1) / chunk));
+          bits_col_count_kernel<<<grid, 256, 0, s>>>(bits, rows, cols, pitch_words, chunk, cc);
+          wg::check_launch("launch column counts");
+        });
+  });
+}
+
+int wg_u8_count(int device, const uint8_t* flags, size_t rows, size_t cols, uint64_t* row_counts,
+                uint64_t* col_counts, uint64_t* total, wg_stream_t stream) {
+  return wg::guarded([&] {
+    wg::DeviceGuard g(device);
+    cudaStream_t s = stream;
+    run_counts(
+        device, rows, cols, row_counts, col_counts, total, s,
+        [&](unsigned long long* tot) {
+          u8_row_count_kernel<<<wg::grid_for(rows * 32, 256, device, 8), 256, 0, s>>>(flags, rows, cols, row_counts,
+                                                                                     tot);
+          wg::check_launch("launch row counts");
+        },
+        [&](unsigned long long* cc) {
+          const size_t chunk = 4096;
+          dim3 grid(static_cast<unsigned>((cols + 255) / 256), static_cast<unsigned>((rows + chunk - 1) / chunk));
+          u8_col_count_kernel<<<grid, 256, 0, s>>>(flags, rows, cols, chunk, cc);
+          wg::check_launch("launch column counts");
+        });
+  });
+}
+
+}  // extern "C"
