@@ -180,6 +180,19 @@ int wg_expect_batched(int device, size_t n_pairs, const wg_expect_plan_t* plans,
                       double* const* term_values, double* const* hpsis,
                       wg_stream_t stream);
 
+/* Prepared batch (new; no reference counterpart): the work tables for fixed
+ * (plan, psi, outputs) pairs are uploaded once; wg_expect_batch_run then only
+ * enqueues kernels on `stream` (no host synchronisation or host copies), so a
+ * run can be captured in a CUDA graph and replayed.  Plans and buffers must
+ * outlive the batch; runs of batches sharing a plan must not overlap. */
+typedef struct wg_expect_batch_s* wg_expect_batch_t;
+int wg_expect_batch_create(int device, size_t n_pairs, const wg_expect_plan_t* plans,
+                           const void* const* psis, int psi_dtype, double* const* results,
+                           double* const* term_values, double* const* hpsis,
+                           wg_expect_batch_t* batch, wg_stream_t stream);
+int wg_expect_batch_run(wg_expect_batch_t batch, wg_stream_t stream);
+int wg_expect_batch_destroy(wg_expect_batch_t batch);
+
 /* <H> over computational-basis counts (PauliSum::expectation_z_counts,
  * src/expectation.cpp:219-247): packed[rows*words] bitstrings (device),
  * counts[rows] (device).  Diagonal terms only.  Result on the host. */

@@ -287,9 +287,12 @@ def test_expectation_cuda_array_interface_and_validation(cuda):
     host = np.zeros(8, np.complex128)
     with pytest.raises(ValueError, match="device memory"):
         op.expectation_statevector(Fake(shape=(8,), typestr="<c16", data=(host.ctypes.data, False), version=3))
+    # 2^36 amplitudes (1 TiB) cannot lie inside the allocation behind a small
+    # tensor: the extent check rejects it on the host, before any kernel runs.
+    wide = PauliSum.from_sparse_list([("Z", [35], 1.0)], num_qubits=36).to_device()
     small = t.zeros(4, dtype=t.complex128, device="cuda")
     with pytest.raises(ValueError, match="backing allocation"):
-        op.expectation_statevector(Fake(shape=(8,), typestr="<c16", data=(small.data_ptr(), False), version=3))
+        wide.expectation_statevector(Fake(shape=(1 << 36,), typestr="<c16", data=(small.data_ptr(), False), version=3))
 
 
 # ---------------------------------------------------------------- DevicePauliSum

@@ -69,6 +69,9 @@ _SIGNATURES: dict[str, list] = {
     "wg_expect_plan_run": [_vp, _vp, _i, _vp, _vp, _vp, _vp],
     "wg_expectation": [_i, _sz, _sz, _vp, _vp, _vp, _vp, _i, ctypes.POINTER(_d), _vp],
     "wg_expect_batched": [_i, _sz, _pvp, _pvp, _i, _pvp, _pvp, _pvp, _vp],
+    "wg_expect_batch_create": [_i, _sz, _pvp, _pvp, _i, _pvp, _pvp, _pvp, _pvp, _vp],
+    "wg_expect_batch_run": [_vp, _vp],
+    "wg_expect_batch_destroy": [_vp],
     "wg_expectation_z_counts": [_i, _sz, _sz, _vp, _vp, _vp, _sz, _vp, _vp, ctypes.POINTER(_d), _vp],
     "wg_group_commuting": [_i, _sz, _sz, _vp, _vp, _i, _psz, _psz, _psz, _vp],
 }

@@ -97,37 +97,47 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Items of pair p span [item_base[p], item_base[p+1]); item -> (group, chunk).
-struct ItemTable {
-  const PlanDev* plans;
-  const uint64_t* item_base;  // [n_plans + 1]
-  const void* const* psis;
-  uint32_t n_plans;
-  unsigned long long* counter;
+// Device work tables of one batched launch (kernel parameter, by value).
+struct BatchDev {
+  const PlanDev* plans;       // [np]
+  const uint64_t* item_base;  // [np+1] forward items (group x chunk) per pair
+  const uint64_t* term_base;  // [np+1] flat term offsets
+  const uint64_t* tile_base;  // [np+1] adjoint tiles (0 for pairs without H psi)
+  const void* const* psis;    // [np]
+  double* const* evals;       // [np] e_k outputs (original order)
+  double* const* results;     // [np] E outputs or null
+  double* const* hpsis;       // [np] H psi outputs or null
+  unsigned long long* counters;  // [2] forward / adjoint work queues
+  uint32_t np;
+  uint64_t n_items, n_terms, n_tiles;
 };
 
+__device__ __forceinline__ uint32_t find_pair(const uint64_t* base, uint32_t np, uint64_t v) {
+  uint32_t lo = 0, hi = np;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (base[mid] <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <typename Amp>
-__global__ void __launch_bounds__(kThreads) expect_forward_kernel(ItemTable tab, uint64_t n_items) {
+__global__ void __launch_bounds__(kThreads) expect_forward_kernel(BatchDev B) {
   __shared__ double red[kThreads / 32][kTermChunk];
   __shared__ uint64_t s_item;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   while (true) {
-    if (threadIdx.x == 0) s_item = atomicAdd(tab.counter, 1ull);
+    if (threadIdx.x == 0) s_item = atomicAdd(B.counters, 1ull);
     __syncthreads();
     const uint64_t item = s_item;
     __syncthreads();
-    if (item >= n_items) break;
-    // plan lookup (few plans: binary search over item_base)
-    uint32_t lo = 0, hi = tab.n_plans;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (tab.item_base[mid] <= item) lo = mid;
-      else hi = mid;
-    }
-    const PlanDev& P = tab.plans[lo];
-    const void* psi = tab.psis[lo];
-    const uint64_t local = item - tab.item_base[lo];
+    if (item >= B.n_items) break;
+    const uint32_t p = find_pair(B.item_base, B.np, item);
+    const PlanDev& P = B.plans[p];
+    const void* psi = B.psis[p];
+    const uint64_t local = item - B.item_base[p];
     const uint32_t g = static_cast<uint32_t>(local / P.C);
     const uint32_t c = static_cast<uint32_t>(local - static_cast<uint64_t>(g) * P.C);
     const uint64_t x = P.gx[g];
@@ -190,9 +200,13 @@ __global__ void __launch_bounds__(kThreads) expect_forward_kernel(ItemTable tab,
 }
 
 // e_k from the chunk partials (summed in chunk order), scaled by the pairing
-// factor and scattered to original term order.
-__global__ void __launch_bounds__(kThreads) expect_finish_terms_kernel(PlanDev P, double* __restrict__ evals) {
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < P.T; k += gridDim.x * blockDim.x) {
+// factor and scattered to original term order; flat over every pair's terms.
+__global__ void __launch_bounds__(kThreads) expect_finish_terms_kernel(BatchDev B) {
+  for (uint64_t f = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; f < B.n_terms;
+       f += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t p = find_pair(B.term_base, B.np, f);
+    const PlanDev& P = B.plans[p];
+    const uint32_t k = static_cast<uint32_t>(f - B.term_base[p]);
     double s = 0.0;
     for (int c = 0; c < P.C; ++c) s += P.partial[static_cast<size_t>(k) * P.C + c];
     const uint32_t ty = P.ty[k];
@@ -207,47 +221,65 @@ __global__ void __launch_bounds__(kThreads) expect_finish_terms_kernel(PlanDev P
         default: e = 2.0 * s; break;
       }
     }
-    evals[P.torig[k]] = e;
+    B.evals[p][P.torig[k]] = e;
   }
 }
 
-__global__ void __launch_bounds__(1024) expect_total_kernel(const double* __restrict__ coeffs,
-                                                            const double* __restrict__ evals, uint32_t T,
-                                                            double* __restrict__ result) {
-  __shared__ double sre[32], sim[32];
-  double re = 0.0, im = 0.0;
-  for (uint32_t k = threadIdx.x; k < T; k += blockDim.x) {
-    re += coeffs[2 * k] * evals[k];
-    im += coeffs[2 * k + 1] * evals[k];
-  }
-  re = warp_sum(re);
-  im = warp_sum(im);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    sre[warp] = re;
-    sim[warp] = im;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-    re = lane < nw ? sre[lane] : 0.0;
-    im = lane < nw ? sim[lane] : 0.0;
+// E_p = sum_k c_k e_k, one block per pair, tree reduction in a fixed order.
+__global__ void __launch_bounds__(kThreads) expect_total_kernel(BatchDev B) {
+  __shared__ double sre[kThreads / 32], sim[kThreads / 32];
+  for (uint32_t p = blockIdx.x; p < B.np; p += gridDim.x) {
+    double* out = B.results[p];
+    if (!out) continue;
+    const PlanDev& P = B.plans[p];
+    const double* ev = B.evals[p];
+    double re = 0.0, im = 0.0;
+    for (uint32_t k = threadIdx.x; k < P.T; k += blockDim.x) {
+      re += P.coeffs[2 * k] * ev[k];
+      im += P.coeffs[2 * k + 1] * ev[k];
+    }
     re = warp_sum(re);
     im = warp_sum(im);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
-      result[0] = re;
-      result[1] = im;
+      sre[warp] = re;
+      sim[warp] = im;
     }
+    __syncthreads();
+    if (warp == 0) {
+      re = lane < kThreads / 32 ? sre[lane] : 0.0;
+      im = lane < kThreads / 32 ? sim[lane] : 0.0;
+      re = warp_sum(re);
+      im = warp_sum(im);
+      if (lane == 0) {
+        out[0] = re;
+        out[1] = im;
+      }
+    }
+    __syncthreads();
   }
 }
 
-// Output-stationary adjoint: thread owns amplitudes j = tile0 + t + 256 r.
+// Output-stationary adjoint over all pairs' tiles (persistent work queue):
+// thread owns amplitudes j = tile0 + t + 256 r of one pair's H psi.
 constexpr int kAdjR = 4;
+constexpr uint64_t kAdjTile = static_cast<uint64_t>(kThreads) * kAdjR;
+
 template <typename Amp>
-__global__ void __launch_bounds__(kThreads) expect_adjoint_kernel(PlanDev P, const void* psi, double* hpsi) {
-  const uint64_t N = uint64_t{1} << P.n;
-  const uint64_t tile = static_cast<uint64_t>(kThreads) * kAdjR;
-  for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * tile; t0 < N; t0 += static_cast<uint64_t>(gridDim.x) * tile) {
+__global__ void __launch_bounds__(kThreads) expect_adjoint_kernel(BatchDev B) {
+  __shared__ uint64_t s_item;
+  while (true) {
+    if (threadIdx.x == 0) s_item = atomicAdd(B.counters + 1, 1ull);
+    __syncthreads();
+    const uint64_t item = s_item;
+    __syncthreads();
+    if (item >= B.n_tiles) break;
+    const uint32_t p = find_pair(B.tile_base, B.np, item);
+    const PlanDev& P = B.plans[p];
+    const void* psi = B.psis[p];
+    double* hpsi = B.hpsis[p];
+    const uint64_t N = uint64_t{1} << P.n;
+    const uint64_t t0 = (item - B.tile_base[p]) * kAdjTile;
     c128 acc[kAdjR];
 #pragma unroll
     for (int r = 0; r < kAdjR; ++r) acc[r] = {0.0, 0.0};
@@ -431,94 +463,158 @@ struct RunSpec {
   double* hpsi;
 };
 
-// Forward pass for any number of (plan, psi) pairs in one persistent launch,
-// then per-pair finishing kernels and (optionally) the adjoint.
-void run_specs(int device, const std::vector<RunSpec>& specs, int dtype, cudaStream_t s) {
-  if (dtype != WG_DTYPE_C128 && dtype != WG_DTYPE_C64)
-    wg::throw_invalid("psi dtype must be complex64 or complex128");
+}  // namespace
+
+// A prepared batch: device work tables for fixed (plan, psi, outputs) pairs.
+// Running it only enqueues kernels (no host synchronisation, no host copies),
+// so a run can be captured in a CUDA graph and replayed.
+struct wg_expect_batch_s {
+  int device = 0;
+  int dtype = WG_DTYPE_C128;
+  int sms = 0;
+  BatchDev dev{};
+  wg::Scratch table;
+  std::vector<wg::Scratch> evtmp;
+};
+
+namespace {
+
+wg_expect_batch_s* make_batch(int device, const std::vector<RunSpec>& specs, int dtype, cudaStream_t s) {
+  if (dtype != WG_DTYPE_C128 && dtype != WG_DTYPE_C64) wg::throw_invalid("psi dtype must be complex64 or complex128");
+  std::unique_ptr<wg_expect_batch_s> b(new wg_expect_batch_s());
+  b->device = device;
+  b->dtype = dtype;
+  b->sms = wg::device_props(device).sm_count;
   const size_t np = specs.size();
+  if (np > 0xffffffffull) wg::throw_invalid("too many pairs in one batch");
   std::vector<PlanDev> plans(np);
-  std::vector<uint64_t> base(np + 1, 0);
+  std::vector<uint64_t> item_base(np + 1, 0), term_base(np + 1, 0), tile_base(np + 1, 0);
   std::vector<const void*> psis(np);
+  std::vector<double*> evals(np), results(np), hpsis(np);
+  b->evtmp.resize(np);
   for (size_t i = 0; i < np; ++i) {
-    plans[i] = specs[i].plan->dev;
+    const PlanDev& P = specs[i].plan->dev;
+    plans[i] = P;
     psis[i] = specs[i].psi;
-    base[i + 1] = base[i] + static_cast<uint64_t>(plans[i].G) * plans[i].C;
-  }
-  const uint64_t n_items = base[np];
-  // temporaries per pair for e_k when the caller does not want them
-  std::vector<wg::Scratch> evtmp(np);
-  std::vector<double*> evals(np);
-  for (size_t i = 0; i < np; ++i) {
+    item_base[i + 1] = item_base[i] + static_cast<uint64_t>(P.G) * P.C;
+    term_base[i + 1] = term_base[i] + P.T;
+    const uint64_t N = uint64_t{1} << P.n;
+    const bool adj = specs[i].hpsi != nullptr;
+    tile_base[i + 1] = tile_base[i] + (adj ? (N + kAdjTile - 1) / kAdjTile : 0);
     if (specs[i].term_values) {
       evals[i] = specs[i].term_values;
     } else {
-      evtmp[i].reset(8 * std::max<uint32_t>(1, plans[i].T), s);
-      evals[i] = evtmp[i].as<double>();
+      b->evtmp[i].reset(8 * std::max<uint32_t>(1, P.T), s);
+      b->evtmp[i].rebind(nullptr);
+      evals[i] = b->evtmp[i].as<double>();
     }
+    results[i] = specs[i].result;
+    hpsis[i] = specs[i].hpsi;
   }
-  if (n_items > 0) {
-    const size_t bytes = sizeof(PlanDev) * np + 8 * (np + 1) + sizeof(void*) * np + 8;
-    wg::Scratch meta(bytes, s);
-    std::vector<unsigned char> host(bytes, 0);
-    std::memcpy(host.data(), plans.data(), sizeof(PlanDev) * np);
-    std::memcpy(host.data() + sizeof(PlanDev) * np, base.data(), 8 * (np + 1));
-    std::memcpy(host.data() + sizeof(PlanDev) * np + 8 * (np + 1), psis.data(), sizeof(void*) * np);
-    wg::check_cuda(cudaMemcpyAsync(meta.get(), host.data(), bytes, cudaMemcpyHostToDevice, s), "upload work table");
-    auto* mb = static_cast<unsigned char*>(meta.get());
-    ItemTable tab;
-    tab.plans = reinterpret_cast<const PlanDev*>(mb);
-    tab.item_base = reinterpret_cast<const uint64_t*>(mb + sizeof(PlanDev) * np);
-    tab.psis = reinterpret_cast<const void* const*>(mb + sizeof(PlanDev) * np + 8 * (np + 1));
-    tab.n_plans = static_cast<uint32_t>(np);
-    tab.counter = reinterpret_cast<unsigned long long*>(mb + bytes - 8);
-    const int sms = wg::device_props(device).sm_count;
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(n_items, static_cast<uint64_t>(sms) * 8));
-    if (dtype == WG_DTYPE_C128)
-      WG_TIMED("expect_forward_kernel", s,
-        expect_forward_kernel<double2><<<grid, kThreads, 0, s>>>(tab, n_items));
+  // one device block: plans | item_base | term_base | tile_base | psis | evals | results | hpsis | counters
+  const size_t bytes = sizeof(PlanDev) * np + 8 * 3 * (np + 1) + 8 * 4 * np + 16;
+  std::vector<unsigned char> host(bytes, 0);
+  size_t off = 0;
+  auto put = [&](const void* src, size_t n) {
+    std::memcpy(host.data() + off, src, n);
+    const size_t at = off;
+    off += n;
+    return at;
+  };
+  const size_t o_plans = put(plans.data(), sizeof(PlanDev) * np);
+  const size_t o_item = put(item_base.data(), 8 * (np + 1));
+  const size_t o_term = put(term_base.data(), 8 * (np + 1));
+  const size_t o_tile = put(tile_base.data(), 8 * (np + 1));
+  const size_t o_psis = put(psis.data(), 8 * np);
+  const size_t o_evals = put(evals.data(), 8 * np);
+  const size_t o_res = put(results.data(), 8 * np);
+  const size_t o_hpsi = put(hpsis.data(), 8 * np);
+  const size_t o_cnt = off;
+  b->table.reset(bytes, s);
+  b->table.rebind(nullptr);
+  // pageable source: the call returns once the bytes are staged
+  wg::check_cuda(cudaMemcpyAsync(b->table.get(), host.data(), bytes, cudaMemcpyHostToDevice, s), "upload work table");
+  auto* base = static_cast<unsigned char*>(b->table.get());
+  BatchDev& d = b->dev;
+  d.plans = reinterpret_cast<const PlanDev*>(base + o_plans);
+  d.item_base = reinterpret_cast<const uint64_t*>(base + o_item);
+  d.term_base = reinterpret_cast<const uint64_t*>(base + o_term);
+  d.tile_base = reinterpret_cast<const uint64_t*>(base + o_tile);
+  d.psis = reinterpret_cast<const void* const*>(base + o_psis);
+  d.evals = reinterpret_cast<double* const*>(base + o_evals);
+  d.results = reinterpret_cast<double* const*>(base + o_res);
+  d.hpsis = reinterpret_cast<double* const*>(base + o_hpsi);
+  d.counters = reinterpret_cast<unsigned long long*>(base + o_cnt);
+  d.np = static_cast<uint32_t>(np);
+  d.n_items = item_base[np];
+  d.n_terms = term_base[np];
+  d.n_tiles = tile_base[np];
+  return b.release();
+}
+
+// Enqueues forward, finish, totals and adjoint; no host synchronisation.
+void run_batch(const wg_expect_batch_s& b, cudaStream_t s) {
+  const BatchDev& d = b.dev;
+  if (d.np == 0) return;
+  wg::check_cuda(cudaMemsetAsync(d.counters, 0, 16, s), "reset work queues");
+  const unsigned persistent = static_cast<unsigned>(b.sms) * 8;
+  if (d.n_items) {
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(d.n_items, persistent));
+    if (b.dtype == WG_DTYPE_C128)
+      WG_TIMED("expect_forward_kernel", s, expect_forward_kernel<double2><<<grid, kThreads, 0, s>>>(d));
     else
-      WG_TIMED("expect_forward_kernel", s,
-        expect_forward_kernel<float2><<<grid, kThreads, 0, s>>>(tab, n_items));
+      WG_TIMED("expect_forward_kernel", s, expect_forward_kernel<float2><<<grid, kThreads, 0, s>>>(d));
     wg::check_launch("launch expectation forward");
-    // keep the table alive until the kernel has run
-    wg::check_cuda(cudaStreamSynchronize(s), "expectation forward");
   }
-  for (size_t i = 0; i < np; ++i) {
-    const PlanDev& P = plans[i];
-    if (P.T > 0) {
-      const unsigned g = wg::grid_for(P.T, kThreads, device, 4);
-      WG_TIMED("expect_finish_terms_kernel", s,
-        expect_finish_terms_kernel<<<g, kThreads, 0, s>>>(P, evals[i]));
-      wg::check_launch("launch expectation finish");
-    }
-    if (specs[i].result) {
-      if (P.T > 0) {
-        WG_TIMED("expect_total_kernel", s,
-          expect_total_kernel<<<1, 1024, 0, s>>>(P.coeffs, evals[i], P.T, specs[i].result));
-        wg::check_launch("launch expectation total");
-      } else {
-        wg::check_cuda(cudaMemsetAsync(specs[i].result, 0, 16, s), "clear expectation");
-      }
-    }
-    if (specs[i].hpsi) {
-      const uint64_t N = uint64_t{1} << P.n;
-      if (P.T == 0) {
-        wg::check_cuda(cudaMemsetAsync(specs[i].hpsi, 0, 16 * N, s), "clear H psi");
-      } else {
-        const uint64_t tiles = (N + kThreads * kAdjR - 1) / (kThreads * kAdjR);
-        const unsigned g = static_cast<unsigned>(std::min<uint64_t>(tiles, wg::device_props(device).sm_count * 8ull));
-        if (dtype == WG_DTYPE_C128)
-          WG_TIMED("expect_adjoint_kernel", s,
-            expect_adjoint_kernel<double2><<<g, kThreads, 0, s>>>(P, specs[i].psi, specs[i].hpsi));
-        else
-          WG_TIMED("expect_adjoint_kernel", s,
-            expect_adjoint_kernel<float2><<<g, kThreads, 0, s>>>(P, specs[i].psi, specs[i].hpsi));
-        wg::check_launch("launch expectation adjoint");
-      }
-    }
+  if (d.n_terms) {
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((d.n_terms + kThreads - 1) / kThreads, persistent));
+    WG_TIMED("expect_finish_terms_kernel", s, expect_finish_terms_kernel<<<grid, kThreads, 0, s>>>(d));
+    wg::check_launch("launch expectation finish");
   }
-  // evtmp buffers are released stream-ordered after the kernels that use them
+  WG_TIMED("expect_total_kernel", s,
+           expect_total_kernel<<<std::min<uint32_t>(d.np, 65535u), kThreads, 0, s>>>(d));
+  wg::check_launch("launch expectation total");
+  if (d.n_tiles) {
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(d.n_tiles, persistent));
+    if (b.dtype == WG_DTYPE_C128)
+      WG_TIMED("expect_adjoint_kernel", s, expect_adjoint_kernel<double2><<<grid, kThreads, 0, s>>>(d));
+    else
+      WG_TIMED("expect_adjoint_kernel", s, expect_adjoint_kernel<float2><<<grid, kThreads, 0, s>>>(d));
+    wg::check_launch("launch expectation adjoint");
+  }
+}
+
+// Pairs whose operator has no terms: E = 0, e = {}, H psi = 0.
+void clear_empty(const std::vector<RunSpec>& specs, cudaStream_t s) {
+  for (const RunSpec& r : specs) {
+    if (r.plan->dev.T != 0) continue;
+    if (r.result) wg::check_cuda(cudaMemsetAsync(r.result, 0, 16, s), "clear expectation");
+    if (r.hpsi) wg::check_cuda(cudaMemsetAsync(r.hpsi, 0, 16ull << r.plan->dev.n, s), "clear H psi");
+  }
+}
+
+void run_specs(int device, const std::vector<RunSpec>& specs, int dtype, cudaStream_t s) {
+  std::unique_ptr<wg_expect_batch_s> b(make_batch(device, specs, dtype, s));
+  clear_empty(specs, s);
+  run_batch(*b, s);
+  // stream-ordered release after the kernels that read the tables
+  b->table.rebind(s);
+  for (auto& e : b->evtmp) e.rebind(s);
+}
+
+std::vector<RunSpec> batch_specs(int device, size_t n_pairs, const wg_expect_plan_t* plans, const void* const* psis,
+                                 double* const* results, double* const* term_values, double* const* hpsis) {
+  std::vector<RunSpec> specs(n_pairs);
+  for (size_t i = 0; i < n_pairs; ++i) {
+    if (!plans[i]) wg::throw_invalid("expectation plan is null");
+    if (plans[i]->h.device != device) wg::throw_invalid("expectation plan belongs to another device");
+    if (!psis[i]) wg::throw_invalid("CUDA statevector data pointer must be non-null");
+    for (size_t j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) wg::throw_invalid("a plan may appear at most once per batched launch");
+    specs[i] = RunSpec{&plans[i]->h, psis[i], results ? results[i] : nullptr, term_values ? term_values[i] : nullptr,
+                       hpsis ? hpsis[i] : nullptr};
+  }
+  return specs;
 }
 
 }  // namespace
@@ -531,9 +627,8 @@ int wg_expect_plan_create(int device, size_t n_qubits, size_t n_terms, const uin
     *plan = nullptr;
     if (n_qubits > 63) wg::throw_invalid("expectation_statevector requires num_qubits <= 63");
     wg::DeviceGuard g(device);
-    wg_plan_host* p = make_plan(device, n_qubits, n_terms, x, z, coeffs, stream);
+    std::unique_ptr<wg_plan_host> p(make_plan(device, n_qubits, n_terms, x, z, coeffs, stream));
     *plan = reinterpret_cast<wg_expect_plan_t>(new wg_expect_plan_s{std::move(*p)});
-    delete p;
   });
 }
 
@@ -601,17 +696,37 @@ int wg_expect_batched(int device, size_t n_pairs, const wg_expect_plan_t* plans,
   return wg::guarded([&] {
     if (n_pairs == 0) return;
     wg::DeviceGuard g(device);
-    std::vector<RunSpec> specs(n_pairs);
-    for (size_t i = 0; i < n_pairs; ++i) {
-      if (!plans[i]) wg::throw_invalid("expectation plan is null");
-      if (plans[i]->h.device != device) wg::throw_invalid("expectation plan belongs to another device");
-      if (!psis[i]) wg::throw_invalid("CUDA statevector data pointer must be non-null");
-      for (size_t j = 0; j < i; ++j)
-        if (plans[j] == plans[i]) wg::throw_invalid("a plan may appear at most once per batched launch");
-      specs[i] = RunSpec{&plans[i]->h, psis[i], results ? results[i] : nullptr,
-                         term_values ? term_values[i] : nullptr, hpsis ? hpsis[i] : nullptr};
-    }
-    run_specs(device, specs, psi_dtype, stream);
+    run_specs(device, batch_specs(device, n_pairs, plans, psis, results, term_values, hpsis), psi_dtype, stream);
+  });
+}
+
+int wg_expect_batch_create(int device, size_t n_pairs, const wg_expect_plan_t* plans, const void* const* psis,
+                           int psi_dtype, double* const* results, double* const* term_values,
+                           double* const* hpsis, wg_expect_batch_t* batch, wg_stream_t stream) {
+  return wg::guarded([&] {
+    *batch = nullptr;
+    wg::DeviceGuard g(device);
+    const auto specs = batch_specs(device, n_pairs, plans, psis, results, term_values, hpsis);
+    for (const RunSpec& r : specs)
+      if (r.plan->dev.T == 0) wg::throw_invalid("a prepared batch needs operators with at least one term");
+    *batch = make_batch(device, specs, psi_dtype, stream);
+    wg::check_cuda(cudaStreamSynchronize(stream), "prepare batch");
+  });
+}
+
+int wg_expect_batch_run(wg_expect_batch_t batch, wg_stream_t stream) {
+  return wg::guarded([&] {
+    if (!batch) wg::throw_invalid("expectation batch is null");
+    wg::DeviceGuard g(batch->device);
+    run_batch(*batch, stream);
+  });
+}
+
+int wg_expect_batch_destroy(wg_expect_batch_t batch) {
+  return wg::guarded([&] {
+    if (!batch) return;
+    wg::DeviceGuard g(batch->device);
+    delete batch;
   });
 }
 
