@@ -188,7 +188,7 @@ def bench_products(args, world, rank, torch) -> dict:
     from wolfgang_b200 import capi
     from wolfgang_b200.workloads import config2
 
-    A, B = config2()
+    A, B = config2(args.lhs_terms, args.rhs_terms)
     n = A[0]
     W = 2
     nl, nr = len(A[3]), len(B[3])
@@ -259,7 +259,8 @@ def bench_products(args, world, rank, torch) -> dict:
         "value": value,
         "unit": "terms/s",
         "ms_per_step": ms_per_step,
-        "config": {"workload": "config2: A(32768)xB(16384) terms, 100 qubits, k-local w in {2,3,4}, matmul+simplify(atol=1e-12)",
+        "config": {"workload": f"config2: A({nl})xB({nr}) terms, 100 qubits, k-local w in {{2,3,4}}, "
+                               "matmul+simplify(atol=1e-12)",
                    "products": P, "survivors": U, "words": W,
                    "l2": "intermediates >> L2 (126 MB); 512 MiB L2 flush between steps",
                    "survey_bytes_per_step": 2 * P * 48 + U * 48,
@@ -331,6 +332,8 @@ def main() -> None:
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--ref-rows", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lhs-terms", type=int, default=32768, help="A terms (smaller values: profiling cases)")
+    ap.add_argument("--rhs-terms", type=int, default=16384, help="B terms")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
