@@ -103,6 +103,23 @@ int wg_bits_to_u8(int device, const uint32_t* bits, size_t rows, size_t cols,
 int wg_bits_count(int device, const uint32_t* bits, size_t rows, size_t cols,
                   size_t pitch_words, uint64_t* row_counts, uint64_t* col_counts,
                   uint64_t* total, wg_stream_t stream);
+/* Dense uint8 commutation flags without any device allocation.  This entry
+ * point has no counterpart in the reference.  It is for callers that cannot
+ * allocate device memory while they run it: a host framework that owns and
+ * accounts for the whole device budget, or a latency-critical loop that must
+ * not call cudaMalloc/cudaFree (they synchronise the device).  The caller
+ * passes the inputs and out[n_lhs*n_rhs]; the bit-packed matrix in between is
+ * kept in one static 32 MiB device array that every GPU loading this library
+ * holds until the process exits.  Limit: n_lhs * ceil(n_rhs/32) * 4 bytes
+ * <= 32 MiB (up to 2^28 entries), larger requests fail with WG_ERR_INVALID.
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU (different
+ * streams or threads) race; serialise them. */
+int wg_commutation_u8_noalloc(int device, size_t words, const uint64_t* lhs_x,
+                              const uint64_t* lhs_z, size_t n_lhs, const uint64_t* rhs_x,
+                              const uint64_t* rhs_z, size_t n_rhs, uint8_t* out,
+                              wg_stream_t stream);
 /* The same counts over a dense uint8 flag matrix (DeviceCommutationMatrix). */
 int wg_u8_count(int device, const uint8_t* flags, size_t rows, size_t cols,
                 uint64_t* row_counts, uint64_t* col_counts, uint64_t* total,

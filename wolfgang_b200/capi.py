@@ -58,6 +58,7 @@ _SIGNATURES: dict[str, list] = {
     "wg_profile_report": [ctypes.c_char_p, _sz],
     "wg_commutation_bits": [_i, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _sz, _i, _vp],
     "wg_bits_to_u8": [_i, _vp, _sz, _sz, _sz, _vp, _vp],
+    "wg_commutation_u8_noalloc": [_i, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp],
     "wg_bits_count": [_i, _vp, _sz, _sz, _sz, _vp, _vp, ctypes.POINTER(ctypes.c_uint64), _vp],
     "wg_u8_count": [_i, _vp, _sz, _sz, _vp, _vp, ctypes.POINTER(ctypes.c_uint64), _vp],
     "wg_simplify": [_i, _sz, _sz, _vp, _vp, _vp, _d, _d, _pvp, _pvp, _pvp, _psz, _vp],

@@ -11,6 +11,8 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "wg_common.cuh"
@@ -478,3 +480,58 @@ int wg_u8_count(int device, const uint8_t* flags, size_t rows, size_t cols, uint
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Commutation flags without any device allocation.
+//
+// Some callers cannot allocate device memory while they use this library: a
+// host framework that owns the whole device budget and accounts for every byte
+// itself, a caller that must not call cudaMalloc/cudaFree in a latency-critical
+// loop (those calls synchronise the device), or a caller that has to keep its
+// memory footprint fixed after start-up.  For them the bit-packed matrix that
+// the ordinary path keeps in a caller or pool buffer lives here instead, in one
+// static device array of kNoAllocScratchBytes.  Every GPU that loads this
+// library holds that array until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t{32} << 20;  // 32 MiB
+static __device__ __align__(256) uint32_t g_noalloc_bits[kNoAllocScratchBytes / sizeof(uint32_t)];
+
+namespace {
+
+// Device address of g_noalloc_bits on `device`, resolved once per device with
+// that device current.  (Host code cannot use the symbol's name as an address.)
+uint32_t* noalloc_scratch(int device) {
+  static std::mutex mu;
+  static std::vector<uint32_t*> addr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (addr.size() <= static_cast<size_t>(device)) addr.resize(device + 1, nullptr);
+  if (!addr[device]) {
+    void* p = nullptr;
+    wg::check_cuda(cudaGetSymbolAddress(&p, g_noalloc_bits), "resolve the no-allocation scratch address");
+    addr[device] = static_cast<uint32_t*>(p);
+  }
+  return addr[device];
+}
+
+}  // namespace
+
+extern "C" int wg_commutation_u8_noalloc(int device, size_t words, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                                         size_t n_lhs, const uint64_t* rhs_x, const uint64_t* rhs_z, size_t n_rhs,
+                                         uint8_t* out, wg_stream_t stream) {
+  int status = wg::guarded([&] {
+    if (n_lhs == 0 || n_rhs == 0) return;
+    const size_t pitch = (n_rhs + 31) / 32;
+    const size_t bytes = wg::checked_mul(wg::checked_mul(n_lhs, pitch, "commutation bit matrix"), 4,
+                                         "commutation bit matrix");
+    if (bytes > kNoAllocScratchBytes)
+      wg::throw_invalid("commutation matrix too large for the no-allocation path: n_lhs * ceil(n_rhs/32) * 4 = " +
+                        std::to_string(bytes) + " bytes exceeds the 32 MiB static scratch");
+    wg::DeviceGuard g(device);
+    uint32_t* bits = noalloc_scratch(device);
+    // The existing entry points do the work; they allocate nothing themselves.
+    int rc = wg_commutation_bits(device, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch, 0, stream);
+    if (rc != WG_OK) throw wg::Error(rc, wg_last_error());
+    rc = wg_bits_to_u8(device, bits, n_lhs, n_rhs, pitch, out, stream);
+    if (rc != WG_OK) throw wg::Error(rc, wg_last_error());
+  });
+  return status;
+}
