@@ -296,6 +296,155 @@ def bench_products(args, world, rank, torch) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- other workloads
+
+def timed_steps(torch, steps, warmup, fn, flush=None):
+    """Per-step CUDA-event timing on the current stream; returns (total ms, profile, launches)."""
+    from wolfgang_b200 import capi
+
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+        if flush is not None:
+            flush()
+    torch.cuda.synchronize()
+    launches0 = capi.kernel_launches()
+    capi.profile_enable(True)
+    capi.profile_report()
+    total = 0.0
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            if flush is not None:
+                flush()
+        torch.cuda.synchronize()
+    capi.profile_enable(False)
+    return total, capi.profile_report(), capi.kernel_launches() - launches0, clocks.summary()
+
+
+def bench_commutation(args, world, rank, torch) -> dict:
+    """Config 3: bit-packed 262,144^2 commutation matrix (128 qubits)."""
+    from wolfgang_b200 import capi
+    from wolfgang_b200.workloads import config3
+
+    n, x, z, _ = config3(args.terms)
+    T = len(x)
+    pitch = (T + 31) // 32
+    dx, dz = dev(torch, x), dev(torch, z)
+    bits = torch.empty(T * pitch, dtype=torch.int32, device="cuda")
+    L = capi.lib()
+    sh = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def step():
+        capi.check(L.wg_commutation_bits(torch.cuda.current_device(), 2, dx.data_ptr(), dz.data_ptr(), T,
+                                         dx.data_ptr(), dz.data_ptr(), T, bits.data_ptr(), pitch, args.algo, sh))
+
+    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, step)
+    t = max_over_ranks(total, world) / args.steps
+    pairs = T * T
+    out_bytes = T * pitch * 4
+    peak, kind = peaks()
+    rl = roofline(prof, {"commute_plane_kernel": out_bytes, "commute_ballot_kernel": out_bytes}, peak, kind)
+    rl["pairs_per_s"] = pairs / (t * 1e-3)
+    out = {"metric": "commutation pairs/s", "value": world * pairs / (t * 1e-3), "unit": "pairs/s", "ms_per_step": t,
+           "config": {"workload": f"config3: {T} terms x {T} terms, 128 qubits, p=0.05, bit-packed matrix",
+                      "output_bytes": out_bytes, "algo": args.algo},
+           "roofline": rl, "gpu_launches": launches, "clocks": clocks,
+           "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import Reference
+
+        ref = Reference()
+        rows = args.cpu_rows
+        t0 = time.perf_counter()
+        ref.commutes(n, (x[:rows], z[:rows]), (x, z))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": rows * T / dt, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                               "sample": f"{rows} rows x {T} terms via reference PauliSum::commutes_with "
+                                         f"(auto CPU dispatch: {ref.cpu_backend()}), {dt:.1f} s"}
+    return out
+
+
+def bench_expectation(args, world, rank, torch) -> dict:
+    """Config 4: 26 qubits (1 GiB psi), 20,000 Hermitian terms in 2,000 x-groups; E + dE/dc + dE/dpsi*."""
+    from wolfgang_b200.expectation import ExpectationPlan
+    from wolfgang_b200.workloads import config4_operator
+
+    n = args.qubits
+    op = config4_operator(n=n)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20261207)
+    psi = torch.randn(1 << n, dtype=torch.complex128, device="cuda", generator=g)
+    psi /= torch.linalg.vector_norm(psi)
+    if args.c64:
+        psi = psi.to(torch.complex64)
+    plan = ExpectationPlan(op)
+    res = torch.empty(2, dtype=torch.float64, device="cuda")
+
+    def step():
+        plan.run(psi, terms=True, hpsi=not args.forward_only)
+
+    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, step)
+    t = max_over_ranks(total, world) / args.steps
+    amp = 16 if psi.dtype == torch.complex128 else 8
+    G = plan.n_groups
+    psi_bytes = (1 << n) * amp
+    peak, kind = peaks()
+    rl = roofline(prof, {"expect_forward_kernel": G * psi_bytes,
+                         "expect_adjoint_kernel": G * psi_bytes + (1 << n) * 16}, peak, kind)
+    del res
+    return {"metric": "E+grad evals/s" if not args.forward_only else "E evals/s", "value": world * 1e3 / t,
+            "unit": "evals/s", "ms_per_step": t,
+            "config": {"workload": f"config4: {n} qubits, {len(op[3])} terms, {G} x-groups, "
+                                   f"{'c64' if args.c64 else 'c128'} psi, forward{'' if args.forward_only else '+adjoint'}",
+                       "survey_bytes_per_step": G * psi_bytes + (0 if args.forward_only else 2 * psi_bytes + G * psi_bytes)},
+            "roofline": rl, "gpu_launches": launches, "clocks": clocks,
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+
+
+def bench_batched(args, world, rank, torch) -> dict:
+    """Config 5: 512 uneven (H, psi) pairs, forward + gradient, batched vs per-call."""
+    from wolfgang_b200.expectation import ExpectationBatch, ExpectationPlan
+    from wolfgang_b200.workloads import config5_operator, config5_pairs
+
+    pairs = config5_pairs(args.pairs)
+    if world > 1:
+        pairs = pairs[rank::world]
+    plans, psis = [], []
+    dtype = torch.complex64 if args.c64 else torch.complex128
+    for n, T, seed in pairs:
+        plans.append(ExpectationPlan(config5_operator(n, T, seed)))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        p = torch.randn(1 << n, dtype=torch.complex128, device="cuda", generator=gen)
+        psis.append((p / torch.linalg.vector_norm(p)).to(dtype))
+    batch = ExpectationBatch(plans, psis, gradients=True)
+    batch.capture()
+
+    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, batch.replay)
+    t = max_over_ranks(total, world) / args.steps
+
+    def per_call():
+        for pl, ps in zip(plans, psis):
+            pl.run(ps, terms=True, hpsi=True)
+
+    pc_total, _, _, _ = timed_steps(torch, max(1, args.steps // 2), 1, per_call)
+    pc = pc_total / max(1, args.steps // 2)
+    npairs = len(pairs) * world
+    return {"metric": "batched E+grad evals/s", "value": npairs / (t * 1e-3), "unit": "evals/s", "ms_per_step": t,
+            "config": {"workload": f"config5: {npairs} uneven (H, psi) pairs, n in [8,24], T log-uniform "
+                                   f"[100,50000], {'c64' if args.c64 else 'c128'}, forward+gradient, one CUDA graph",
+                       "per_call_evals_per_s": len(pairs) / (pc * 1e-3), "per_call_ms": pc,
+                       "batched_over_per_call": pc / t},
+            "gpu_launches": launches, "clocks": clocks,
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+
+
 def reference_arm(args, world, rank) -> dict:
     """Times the reference's own CPU core on bounded samples of the same workload."""
     from wolfgang_b200.workloads import config2
@@ -327,7 +476,13 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["products"], default="products")
+    ap.add_argument("--workload", choices=["products", "commutation", "expectation", "batched"], default="products")
+    ap.add_argument("--terms", type=int, default=262144, help="commutation terms (config 3)")
+    ap.add_argument("--algo", type=int, default=0, help="commutation algorithm: 0 auto, 1 ballot, 2 bit-plane")
+    ap.add_argument("--qubits", type=int, default=26, help="expectation qubits (config 4)")
+    ap.add_argument("--c64", action="store_true", help="complex64 statevector storage")
+    ap.add_argument("--forward-only", action="store_true")
+    ap.add_argument("--pairs", type=int, default=512, help="batched pairs (config 5)")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--ref-rows", type=int, default=256)
@@ -352,9 +507,12 @@ def main() -> None:
 
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    out = bench_products(args, world, rank, torch)
+    fn = {"products": bench_products, "commutation": bench_commutation, "expectation": bench_expectation,
+          "batched": bench_batched}[args.workload]
+    out = fn(args, world, rank, torch)
     out.update(n_gpus=world, steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling="weak",
-               vs_baseline=None, dtype="f64", data="synthetic (seeded generator of config 2)")
+               vs_baseline=None, dtype="u64" if args.workload == "commutation" else "f64",
+               data=f"synthetic (seeded generator, workload {args.workload})")
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
