@@ -156,6 +156,22 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
                       double rtol, uint64_t** out_x, uint64_t** out_z,
                       double** out_coeffs, size_t* out_terms, wg_stream_t stream);
 
+/* Sort-reduce algorithm behind wg_simplify and the simplifying modes of
+ * wg_pauli_products.  No reference counterpart (the reference has one sort);
+ * both algorithms give identical results, bit for bit.
+ *   WG_SORT_AUTO    (default) bucketed for 1-2 mask words and >= 2^20 items;
+ *   WG_SORT_LSD     multi-word LSD radix sort of full keys;
+ *   WG_SORT_BUCKET  bucketed sort on 64-bit key codes (1-2 mask words, at most
+ *                   255 significant key bits); falls back to WG_SORT_LSD when a
+ *                   bucket exceeds its capacity.
+ * The setting is process-wide.  wg_last_sort_algorithm returns the algorithm
+ * that produced the calling thread's last result (0 before any). */
+#define WG_SORT_AUTO 0
+#define WG_SORT_LSD 1
+#define WG_SORT_BUCKET 2
+int wg_set_sort_algorithm(int algo);
+int wg_last_sort_algorithm(void);
+
 /* -------------------------------------------------------- expectation ---- */
 /* <psi|H|psi> (PauliSum::expectation_statevector_complex{128,64},
  * include/wolfgang/pauli_sum.hpp:91-94; DevicePauliSum::expectation_statevector_*

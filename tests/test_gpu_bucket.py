@@ -1,0 +1,210 @@
+"""Bucketed sort-reduce (WG_SORT_BUCKET) against the oracle and the LSD path.
+
+Both algorithms must give the same bits: keys, order and coefficients.  Cases
+cover dense codes (at most 64 significant bits left in a bucket), position
+codes with tie runs, long runs of one key, fine buckets over capacity (which
+fall back to the LSD path), more than 255 significant bits (not eligible),
+and infinite / NaN coefficients with both threshold modes.
+"""
+
+from __future__ import annotations
+
+import zlib
+
+import numpy as np
+import pytest
+
+from tests import gpu_util as G
+from tests.conftest import random_operator
+from wolfgang_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def seeded(*key):
+    return np.random.default_rng(zlib.crc32(repr(key).encode()))
+
+
+def same(a, b):
+    return all(np.ascontiguousarray(x).tobytes() == np.ascontiguousarray(y).tobytes() and x.shape == y.shape
+               for x, y in zip(a, b))
+
+
+def eligible(*xz):
+    """1 to 255 significant key bits: the bucketed path's precondition."""
+    total = 0
+    for a in xz:
+        a = np.asarray(a, np.uint64).reshape(len(a), -1)
+        for w in range(a.shape[1]):
+            total += bin(int(np.bitwise_or.reduce(a[:, w]) if len(a) else 0)).count("1")
+    return 1 <= total <= 255
+
+
+@pytest.fixture
+def algo():
+    """Sets the sort algorithm for one test and restores WG_SORT_AUTO after it."""
+    def set_(a):
+        capi.set_sort_algorithm(a)
+    yield set_
+    capi.set_sort_algorithm(capi.WG_SORT_AUTO)
+
+
+def klocal(rng, n, T, weights=(2, 3, 4)):
+    from wolfgang_b200.workloads import klocal_operator
+
+    return klocal_operator(rng, n, T, weights)
+
+
+SIMPLIFY_CASES = [
+    (1, 50, 0.5, 4, 0.0, 0.0),
+    (5, 300, 0.3, None, 1e-12, 0.0),
+    (20, 5000, 0.25, 600, 1e-12, 0.0),
+    (20, 100000, 0.25, 3000, 1e-12, 0.0),
+    (64, 2000, 0.1, 300, 0.5, 0.0),
+    (65, 4500, 0.05, 500, 1e-12, 0.01),
+    (100, 30000, 0.04, None, 0.0, 0.0),
+    (100, 60000, 0.08, 7000, 1e-12, 0.0),
+    (127, 20000, 0.03, 2000, 1e-12, 0.5),
+]
+
+
+@pytest.mark.parametrize("case", SIMPLIFY_CASES)
+def test_bucket_simplify_bit_exact(cuda, oracle, algo, case):
+    n, T, p, pool, atol, rtol = case
+    rng = seeded("bucket-simplify", case)
+    _, x, z, c = random_operator(rng, n, T, p, pool)
+    algo(capi.WG_SORT_BUCKET)
+    got = G.simplify(n, x, z, c, atol, rtol)
+    if eligible(x, z):
+        assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    assert same(got, oracle.simplify(n, x, z, c, atol, rtol))
+    algo(capi.WG_SORT_LSD)
+    assert same(got, G.simplify(n, x, z, c, atol, rtol))
+    assert capi.last_sort_algorithm() == capi.WG_SORT_LSD
+
+
+MATMUL_CASES = [
+    (3, 8, 9, 0.5, None, None),
+    (12, 200, 150, 0.3, None, None),
+    (12, 300, 200, 0.3, 40, None),
+    (20, 256, 256, 0.25, None, None),
+    (70, 200, 180, 0.05, 30, None),
+    (100, 2048, 1024, 0.03, None, None),
+    (128, 300, 400, 0.04, None, 50),
+]
+
+
+@pytest.mark.parametrize("case", MATMUL_CASES)
+@pytest.mark.parametrize("mode", [capi.WG_PRODUCTS_SIMPLIFY, capi.WG_PRODUCTS_FUSED])
+def test_bucket_products_bit_exact(cuda, oracle, algo, case, mode):
+    n, nl, nr, p, pl, pr = case
+    rng = seeded("bucket-matmul", case)
+    A = random_operator(rng, n, nl, p, pl)
+    B = random_operator(rng, n, nr, p, pr)
+    algo(capi.WG_SORT_BUCKET)
+    got = G.products(n, A[1:], B[1:], mode)
+    if eligible(A[1], A[2], B[1], B[2]):
+        assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    raw = oracle.matmul(n, A[1:], B[1:], simplify=False)
+    assert same(got, oracle.simplify(n, *raw, 1e-12, 0.0))
+
+
+def test_bucket_klocal_products_match_lsd(cuda, oracle, algo):
+    """A scaled-down config-2 product (100 qubits, k-local terms): position codes."""
+    rng = seeded("bucket-klocal")
+    A = klocal(rng, 100, 2048)
+    B = klocal(rng, 100, 1024)
+    algo(capi.WG_SORT_BUCKET)
+    got = G.products(100, A[1:], B[1:])
+    assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    algo(capi.WG_SORT_LSD)
+    assert same(got, G.products(100, A[1:], B[1:]))
+    raw = oracle.matmul(100, A[1:], B[1:], simplify=False)
+    assert same(got, oracle.simplify(100, *raw, 1e-12, 0.0))
+
+
+def test_bucket_config1_hh_auto(cuda, oracle, algo):
+    """H@H of config 1 (2^24 products) takes the bucketed path by default."""
+    from wolfgang_b200.workloads import config1
+
+    (n, x, z, c), _ = config1()
+    algo(capi.WG_SORT_AUTO)
+    got = G.products(n, (x, z, c), (x, z, c), capi.WG_PRODUCTS_SIMPLIFY)
+    assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    assert same(got, oracle.matmul(n, (x, z, c), (x, z, c), simplify=True))
+
+
+def test_bucket_tie_heavy_position_codes(cuda, oracle, algo):
+    """High-weight terms over 120 qubits: many keys share their first eight set
+    bits, so position codes tie; results stay exact (bucketed or fallen back)."""
+    rng = seeded("bucket-ties")
+    A = random_operator(rng, 120, 400, 0.15)
+    B = random_operator(rng, 120, 300, 0.15)
+    algo(capi.WG_SORT_BUCKET)
+    got = G.products(120, A[1:], B[1:])
+    raw = oracle.matmul(120, A[1:], B[1:], simplify=False)
+    assert same(got, oracle.simplify(120, *raw, 1e-12, 0.0))
+
+
+@pytest.mark.parametrize("copies,bucketed", [(3500, True), (5000, False)])
+def test_bucket_one_key_runs(cuda, oracle, algo, copies, bucketed):
+    """One key repeated: one fine bucket (at most 4096 items) or a fallback."""
+    rng = seeded("bucket-run", copies)
+    n = 40
+    x = np.zeros((copies + 300, 1), np.uint64)
+    z = np.zeros((copies + 300, 1), np.uint64)
+    x[:copies, 0] = np.uint64(0x5A5A5)
+    z[:copies, 0] = np.uint64(0x33)
+    x[copies:, 0] = rng.integers(0, 1 << 40, size=300, dtype=np.uint64)
+    c = rng.normal(size=copies + 300) + 1j * rng.normal(size=copies + 300)
+    perm = rng.permutation(copies + 300)
+    x, z, c = x[perm], z[perm], c[perm]
+    algo(capi.WG_SORT_BUCKET)
+    got = G.simplify(n, x, z, c)
+    assert capi.last_sort_algorithm() == (capi.WG_SORT_BUCKET if bucketed else capi.WG_SORT_LSD)
+    assert same(got, oracle.simplify(n, x, z, c))
+
+
+def test_bucket_not_eligible_above_255_bits(cuda, oracle, algo):
+    rng = seeded("bucket-256")
+    n, x, z, c = random_operator(rng, 128, 3000, 0.5)
+    algo(capi.WG_SORT_BUCKET)
+    got = G.simplify(n, x, z, c)
+    assert capi.last_sort_algorithm() == capi.WG_SORT_LSD
+    assert same(got, oracle.simplify(n, x, z, c))
+
+
+@pytest.mark.parametrize("rtol", [0.0, 0.25])
+def test_bucket_nonfinite_and_cancellation(cuda, oracle, algo, rtol):
+    rng = seeded("bucket-nonfinite", rtol)
+    n, x, z, c = random_operator(rng, 30, 6000, 0.2, 400)
+    c[1::11] = -c[0::11][: len(c[1::11])]
+    c[::13] = 1e-12
+    algo(capi.WG_SORT_BUCKET)
+    for bad in (None, np.inf, np.nan, complex(1e308, 1e308)):
+        cc = c.copy()
+        if bad is not None:
+            cc[17] = bad
+        got = G.simplify(n, x, z, cc, 1e-12, rtol)
+        assert same(got, oracle.simplify(n, x, z, cc, 1e-12, rtol))
+        A = (x[:90], z[:90], cc[:90])
+        B = (x[90:190], z[90:190], cc[90:190].copy())
+        gotp = G.products(n, A, B, capi.WG_PRODUCTS_SIMPLIFY, 1e-12, rtol)
+        raw = oracle.matmul(n, A, B, simplify=False)
+        assert same(gotp, oracle.simplify(n, *raw, 1e-12, rtol))
+
+
+def test_bucket_everything_cancels(cuda, oracle, algo):
+    rng = seeded("bucket-cancel")
+    _, x, z, c = random_operator(rng, 50, 3000, 0.1)
+    x2, z2, c2 = np.concatenate([x, x]), np.concatenate([z, z]), np.concatenate([c, -c])
+    algo(capi.WG_SORT_BUCKET)
+    got = G.simplify(50, x2, z2, c2)
+    assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    assert len(got[2]) == 0
+    assert same(got, oracle.simplify(50, x2, z2, c2))
+
+
+def test_sort_algorithm_rejects_unknown(cuda):
+    with pytest.raises(ValueError):
+        capi.set_sort_algorithm(7)

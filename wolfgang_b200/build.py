@@ -43,7 +43,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall",
              "-I", str(INCLUDE), "-I", str(HOST)]
 
-CU_SOURCES = ["wg_runtime.cu", "wg_commute.cu", "wg_simplify.cu", "wg_expect.cu", "wg_group.cu"]
+CU_SOURCES = ["wg_runtime.cu", "wg_commute.cu", "wg_simplify.cu", "wg_bucket.cu", "wg_expect.cu", "wg_group.cu"]
 CU_HEADERS = ["wg_common.cuh", "wg_scan.cuh"]
 HOST_SOURCES = ["pauli_sum.cpp", "device.cpp"]
 HOST_HEADERS = ["abi.hpp", "guards.hpp"]

@@ -28,6 +28,9 @@ WG_DTYPE_C64 = 1
 WG_PRODUCTS_RAW = 0
 WG_PRODUCTS_SIMPLIFY = 1
 WG_PRODUCTS_FUSED = 2
+WG_SORT_AUTO = 0
+WG_SORT_LSD = 1
+WG_SORT_BUCKET = 2
 
 _sz = ctypes.c_size_t
 _vp = ctypes.c_void_p
@@ -63,6 +66,8 @@ _SIGNATURES: dict[str, list] = {
     "wg_u8_count": [_i, _vp, _sz, _sz, _vp, _vp, ctypes.POINTER(ctypes.c_uint64), _vp],
     "wg_simplify": [_i, _sz, _sz, _vp, _vp, _vp, _d, _d, _pvp, _pvp, _pvp, _psz, _vp],
     "wg_pauli_products": [_i, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _sz, _i, _d, _d, _pvp, _pvp, _pvp, _psz, _vp],
+    "wg_set_sort_algorithm": [_i],
+    "wg_last_sort_algorithm": [],
     "wg_expect_plan_create": [_i, _sz, _sz, _vp, _vp, _vp, _pvp, _vp],
     "wg_expect_plan_destroy": [_vp],
     "wg_expect_plan_set_coeffs": [_vp, _vp, _vp],
@@ -140,6 +145,22 @@ def profile_report() -> dict[str, tuple[int, float]]:
             name, count, ms = item.rsplit(":", 2)
             out[name] = (int(count), float(ms))
     return out
+
+
+def set_sort_algorithm(algo: int) -> int:
+    """Selects the sort-reduce algorithm (WG_SORT_*) process-wide; returns the previous one."""
+    prev = _sort_setting[0]
+    check(lib().wg_set_sort_algorithm(int(algo)))
+    _sort_setting[0] = int(algo)
+    return prev
+
+
+def last_sort_algorithm() -> int:
+    """WG_SORT_LSD or WG_SORT_BUCKET: the algorithm of this thread's last simplify / products result."""
+    return int(lib().wg_last_sort_algorithm())
+
+
+_sort_setting = [WG_SORT_AUTO]
 
 
 def kernel_launches() -> int:

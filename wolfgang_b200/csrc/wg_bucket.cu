@@ -1,0 +1,1516 @@
+// wg_bucket.cu -- bucketed sort-reduce for products and simplify (1 or 2 mask words).
+//
+// Same results as the LSD pipeline of wg_simplify.cu (equal keys summed in
+// input-index order, glibc-exact cull, canonical key order) with far less data
+// movement.  An item is only its 32-bit index (a product l*n_r + r, or an input
+// term); its key and coefficient are recomputed from the packed operands, which
+// stay in L2, whenever they are needed.
+//
+// Compressed keys.  The significant bits (the OR of all keys) are numbered by
+// rank from the most significant end (word 0, bit 63 first).  A key compressed
+// to its significant bits, rank r at bit 63 - r%64 of word r/64, orders like the
+// key itself (the other bits are zero in every key).  Compression is linear
+// over XOR, so a product's compressed key is the XOR of its factors'.
+//
+// Codes.  Items of one bucket share their first L ranks.  The 64-bit code of a
+// compressed key relative to L is
+//   dense     (when at most 64 ranks remain): bits L .. L+63 -- exact;
+//   position  (otherwise): one byte per set bit of rank >= L, the first eight
+//             of them, each 255 - (rank - L), padded with zero bytes.
+// Both agree with the key order wherever codes differ (a < b implies
+// code(a) <= code(b)), so a partition of items by code ranges is a partition
+// by key ranges, and the common prefix of a code range gives the L of the
+// bucket below it.  Equal position codes are told apart by the next eight set
+// bits, then, rarely, by the full key.
+//
+//  coarse  sample codes (L = 0), sort, pick splitters; each item finds its
+//          coarse bucket by binary search over the splitters in shared memory
+//          and its index is scattered into that bucket's region;
+//  fine    one CTA per coarse bucket: sample in-bucket codes, sort them in
+//          shared memory, pick fine splitters (a heavily repeated code gets a
+//          bucket of its own), count, then write (code relative to the fine
+//          bucket's L, index) in fine order;
+//  final   fine buckets in global order, at most kCap items each: shared-memory
+//          merge sort by (code, index), tie runs reordered by (next code,
+//          index) and if need be by (key, index), equal-key runs summed left to
+//          right and culled, survivors written at an offset from a decoupled
+//          look-back over the preceding buckets.  A bucket of one key of any
+//          size has its indices radix-sorted in global memory instead.
+//
+// Anything outside this path's limits (more than 255 significant bits, a
+// coarse region or fine bucket over capacity, a tie of more than 16 different
+// keys) makes the driver return false and the caller runs the LSD pipeline.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "wg_common.cuh"
+
+namespace {
+
+using wgd::c128;
+
+constexpr int kCoarseLog = 18;           // about 2^18 items per coarse bucket
+constexpr int kCoarseMax = 2048;         // coarse buckets
+constexpr int kCoarseSample = 128;       // samples per coarse bucket
+constexpr int kFineAvg = 1536;           // target items per fine bucket
+constexpr int kFineMax = 512;            // target fine buckets per coarse bucket
+constexpr int kFineSlots = 1024;         // fine bucket slots per coarse bucket (targets + isolated codes)
+constexpr int kSample2 = 4096;           // in-bucket sample for fine splitters
+constexpr int kHeavyRun = 3;             // sample repeats that may isolate a code
+constexpr int kK1Threads = 512;
+constexpr int kK1Items = 16;
+constexpr int kK2Threads = 512;
+constexpr int kK3Threads = 256;
+constexpr int kIPT = 16;                        // items per thread in the final sort
+constexpr int kCap = kK3Threads * kIPT;         // 4096 items per fine bucket
+constexpr int kPadded = kCap + kCap / 16;       // one spare slot per 16 (bank spread)
+constexpr int kWords = kCap / 32;
+constexpr int kMaxRuns = kCap / 2;              // tie runs per bucket (runs have >= 2 items)
+constexpr int kDistinct = 16;                   // distinct keys in one tie of 16-digit codes
+constexpr uint32_t kExactBit = 1u << 31;        // fine bucket codes are exact (equal code = equal key)
+constexpr uint32_t kPureBit = 1u << 30;         // every key of the fine bucket is equal
+constexpr uint32_t kCountMask = kPureBit - 1;
+constexpr unsigned kFlagTimeout = 2u;
+constexpr unsigned kFlagOverrun = 4u;           // an output rank beyond capacity (internal error)
+constexpr unsigned kFlagCoarseFull = 8u;        // fallbacks: a coarse region over capacity,
+constexpr unsigned kFlagFineFull = 16u;         //   a fine bucket over kCap items (not of one key),
+constexpr unsigned kFlagDistinct = 32u;         //   a tie of more than kDistinct keys
+constexpr unsigned kFallbackMask = kFlagCoarseFull | kFlagFineFull | kFlagDistinct;
+constexpr unsigned kSpinLimit = 1u << 22;       // look-back polls (~0.5 s with back-off)
+constexpr unsigned long long kStAgg = 1ull << 62;
+constexpr unsigned long long kStIncl = 2ull << 62;
+constexpr unsigned long long kStValue = (1ull << 62) - 1;
+
+struct Control {
+  unsigned k2_ticket;
+  unsigned k3_ticket;
+  unsigned flags;
+  unsigned inf_seen;
+  unsigned long long max_bits;
+  double thr;
+  unsigned long long survivors;
+  unsigned fine_total;
+  unsigned max_fine;  // largest fine bucket
+};
+
+// ------------------------------------------------------------------ keys and codes
+
+template <int KW>
+__device__ __forceinline__ bool keq(const uint64_t (&a)[KW], const uint64_t (&b)[KW]) {
+  bool e = true;
+#pragma unroll
+  for (int i = 0; i < KW; ++i) e = e && (a[i] == b[i]);
+  return e;
+}
+
+template <int KW>
+__device__ __forceinline__ bool kless(const uint64_t (&a)[KW], const uint64_t (&b)[KW]) {
+#pragma unroll
+  for (int i = 0; i < KW; ++i)
+    if (a[i] != b[i]) return a[i] < b[i];
+  return false;
+}
+
+// Bits L .. L+63 of a compressed key (zero past its end).
+template <int KW>
+__device__ __forceinline__ uint64_t window64(const uint64_t (&c)[KW], int L) {
+  const int w = L >> 6, s = L & 63;
+  uint64_t hi = 0, lo = 0;
+#pragma unroll
+  for (int i = 0; i < KW; ++i) {
+    if (i == w) hi = c[i];
+    if (i == w + 1) lo = c[i];
+  }
+  return s == 0 ? hi : (hi << s) | (lo >> (64 - s));
+}
+
+// Position digits skip .. skip+7 of the set bits of rank >= L.
+template <int KW>
+__device__ __forceinline__ uint64_t position_code(const uint64_t (&c)[KW], int L, int skip) {
+  uint64_t code = 0;
+  int nd = 0;
+#pragma unroll
+  for (int w = 0; w < KW; ++w) {
+    const int r0 = 64 * w;
+    uint64_t v = c[w];
+    if (L >= r0 + 64) v = 0;
+    else if (L > r0) v &= ~0ull >> (L - r0);
+    while (v && nd < skip + 8) {
+      const int b = __clzll(v);
+      v &= ~(0x8000000000000000ull >> b);
+      if (nd >= skip) code |= static_cast<uint64_t>(255 - (r0 + b - L)) << (56 - 8 * (nd - skip));
+      ++nd;
+    }
+  }
+  return code;
+}
+
+template <int KW>
+__device__ __forceinline__ uint64_t code_of(const uint64_t (&c)[KW], int L, bool dense) {
+  return dense ? window64<KW>(c, L) : position_code<KW>(c, L, 0);
+}
+
+__device__ __forceinline__ bool dense_at(int total, int L) { return total - L <= 64; }
+
+// Ranks shared by every key whose code (relative to L) lies in [lo, hi].
+__device__ __forceinline__ int child_prefix(int L, bool dense, int total, uint64_t lo, uint64_t hi) {
+  const uint64_t d = lo ^ hi;
+  if (dense) return min(total, L + (d ? __clzll(d) : 64));
+  const int m = d ? (__clzll(d) >> 3) : 8;
+  int Lc = L;
+  for (int q = 0; q < m; ++q) {
+    const int digit = static_cast<int>((lo >> (56 - 8 * q)) & 0xffu);
+    if (digit == 0) return total;  // no further set bits: the keys are equal
+    Lc = L + (255 - digit) + 1;
+  }
+  return min(Lc, total);
+}
+
+// Code range [lo, hi] of bucket j under ns sorted splitters (bucket j holds
+// codes c with split[j-1] <= c < split[j]); false when it is empty.
+__device__ __forceinline__ bool bucket_range(const uint64_t* split, int ns, int j, uint64_t& lo, uint64_t& hi) {
+  lo = j > 0 ? split[j - 1] : 0ull;
+  if (j < ns) {
+    if (split[j] == 0ull) return false;
+    hi = split[j] - 1;
+  } else {
+    hi = ~0ull;
+  }
+  return lo <= hi;
+}
+
+__device__ __forceinline__ int upper_bound_u64(const uint64_t* a, int n, uint64_t v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (v < a[mid]) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Rank of this lane's value among equal values of the warp, via one shared
+// memory atomic per distinct value: returns old counter + rank among peers.
+__device__ __forceinline__ unsigned warp_aggregated_add(unsigned* counters, unsigned key, bool valid) {
+  const unsigned mask = __activemask();
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned k = valid ? key : 0xffffffffu;
+  const unsigned peers = __match_any_sync(mask, k);
+  const int leader = __ffs(peers) - 1;
+  unsigned base = 0;
+  if (valid && static_cast<int>(lane) == leader) base = atomicAdd(&counters[key], __popc(peers));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+// ------------------------------------------------------------------ item sources
+
+// Exact quotient p / d for p, d < 2^32: m = ceil(2^64 / d), and the error of
+// p*m / 2^64 stays below 2^-32 <= 1/d, under the gap to the next integer.
+struct FastDiv {
+  uint32_t d;
+  uint64_t m;
+  __device__ __forceinline__ uint32_t div(uint32_t p) const {
+    return d == 1 ? p : static_cast<uint32_t>(__umul64hi(static_cast<uint64_t>(p), m));
+  }
+};
+
+// Products p = a*nb + b of two packed operands (rhs acts first).
+template <int KW>
+struct ProdSrc {
+  const uint64_t* ak;  // [na][KW]: x0, z0, x1, z1
+  const uint64_t* bk;  // [nb][KW]
+  const uint64_t* ac2; // [na][KW] compressed keys
+  const uint64_t* bc2; // [nb][KW]
+  const double* ac;
+  const double* bc;
+  const uint8_t* ay;   // popc(x & z) mod 4 of each term
+  const uint8_t* by;
+  FastDiv nb;
+
+  __device__ __forceinline__ void ckey(uint32_t p, uint64_t (&c)[KW]) const {
+    const uint32_t a = nb.div(p), b = p - a * nb.d;
+    const uint64_t* pa = ac2 + static_cast<size_t>(a) * KW;
+    const uint64_t* pb = bc2 + static_cast<size_t>(b) * KW;
+#pragma unroll
+    for (int i = 0; i < KW; ++i) c[i] = __ldg(pa + i) ^ __ldg(pb + i);
+  }
+  __device__ __forceinline__ void key(uint32_t p, uint64_t (&k)[KW]) const {
+    const uint32_t a = nb.div(p), b = p - a * nb.d;
+    const uint64_t* pa = ak + static_cast<size_t>(a) * KW;
+    const uint64_t* pb = bk + static_cast<size_t>(b) * KW;
+#pragma unroll
+    for (int i = 0; i < KW; ++i) k[i] = __ldg(pa + i) ^ __ldg(pb + i);
+  }
+  __device__ __forceinline__ c128 key_coeff(uint32_t p, uint64_t (&k)[KW]) const {
+    const uint32_t a = nb.div(p), b = p - a * nb.d;
+    const uint64_t* pa = ak + static_cast<size_t>(a) * KW;
+    const uint64_t* pb = bk + static_cast<size_t>(b) * KW;
+    unsigned e = 8u - __ldg(ay + a) - __ldg(by + b);
+#pragma unroll
+    for (int i = 0; i < KW; i += 2) {
+      const uint64_t axw = __ldg(pa + i), azw = __ldg(pa + i + 1);
+      const uint64_t bxw = __ldg(pb + i), bzw = __ldg(pb + i + 1);
+      k[i] = axw ^ bxw;
+      k[i + 1] = azw ^ bzw;
+      e += __popcll(k[i] & k[i + 1]) + 2u * __popcll(axw & bzw);
+    }
+    const c128 ca{__ldg(ac + 2 * a), __ldg(ac + 2 * a + 1)};
+    const c128 cb{__ldg(bc + 2 * b), __ldg(bc + 2 * b + 1)};
+    return wgd::rotate(wgd::cmul(ca, cb), e);
+  }
+};
+
+// Input terms of simplify.
+template <int KW>
+struct TermSrc {
+  const uint64_t* tk;  // [n][KW]
+  const uint64_t* tc2; // [n][KW] compressed keys
+  const double* c;
+
+  __device__ __forceinline__ void ckey(uint32_t p, uint64_t (&k)[KW]) const {
+    const uint64_t* pt = tc2 + static_cast<size_t>(p) * KW;
+#pragma unroll
+    for (int i = 0; i < KW; ++i) k[i] = __ldg(pt + i);
+  }
+  __device__ __forceinline__ void key(uint32_t p, uint64_t (&k)[KW]) const {
+    const uint64_t* pt = tk + static_cast<size_t>(p) * KW;
+#pragma unroll
+    for (int i = 0; i < KW; ++i) k[i] = __ldg(pt + i);
+  }
+  __device__ __forceinline__ c128 key_coeff(uint32_t p, uint64_t (&k)[KW]) const {
+    key(p, k);
+    return {__ldg(c + 2 * p), __ldg(c + 2 * p + 1)};
+  }
+};
+
+// ------------------------------------------------------------------ packing
+
+// AoS keys [t][2W] in significance order, y = popc(x & z) mod 4, and the OR of
+// every key word into sig.
+__global__ void bucket_pack_kernel(const uint64_t* __restrict__ x, const uint64_t* __restrict__ z, size_t T, int W,
+                                   uint64_t* __restrict__ keys, uint8_t* __restrict__ y,
+                                   unsigned long long* __restrict__ sig) {
+  uint64_t acc[4] = {0, 0, 0, 0};
+  for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < T;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    unsigned yy = 0;
+    for (int w = 0; w < W; ++w) {
+      const uint64_t xv = x[t * W + w], zv = z[t * W + w];
+      keys[t * 2 * W + 2 * w] = xv;
+      keys[t * 2 * W + 2 * w + 1] = zv;
+      acc[2 * w] |= xv;
+      acc[2 * w + 1] |= zv;
+      yy += __popcll(xv & zv);
+    }
+    if (y) y[t] = static_cast<uint8_t>(yy & 3u);
+  }
+  for (int i = 0; i < 2 * W; ++i) {
+    uint64_t v = acc[i];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicOr(sig + i, static_cast<unsigned long long>(v));
+  }
+}
+
+struct SigWords {
+  uint64_t w[4];
+};
+
+// Compressed keys [t][KW] of packed keys [t][KW] under the significant bits.
+__global__ void bucket_compress_kernel(const uint64_t* __restrict__ keys, size_t T, int KW, SigWords sig,
+                                       uint64_t* __restrict__ out) {
+  for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < T;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    uint64_t c[4] = {0, 0, 0, 0};
+    int base = 0;
+    for (int w = 0; w < KW; ++w) {
+      uint64_t m = keys[t * KW + w] & sig.w[w];
+      while (m) {
+        const int b = 63 - __clzll(m);
+        m ^= uint64_t{1} << b;
+        const int r = base + __popcll(sig.w[w] & ~((uint64_t{2} << b) - 1));
+        c[r >> 6] |= 0x8000000000000000ull >> (r & 63);
+      }
+      base += __popcll(sig.w[w]);
+    }
+    for (int w = 0; w < KW; ++w) out[t * KW + w] = c[w];
+  }
+}
+
+// ------------------------------------------------------------------ coarse splitters
+
+// splitmix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom
+// number generators", OOPSLA 2014).
+__device__ __forceinline__ uint64_t mix64(uint64_t v) {
+  v += 0x9e3779b97f4a7c15ull;
+  v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ull;
+  v = (v ^ (v >> 27)) * 0x94d049bb133111ebull;
+  return v ^ (v >> 31);
+}
+
+template <int KW, class Src>
+__global__ void bucket_sample_kernel(Src src, uint32_t n, uint32_t S, bool dense, uint64_t* __restrict__ codes,
+                                     uint32_t* __restrict__ idx) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S; i += gridDim.x * blockDim.x) {
+    const uint32_t p = S >= n ? i : static_cast<uint32_t>(__umul64hi(mix64(i), static_cast<uint64_t>(n)));
+    uint64_t c[KW];
+    src.ckey(p, c);
+    codes[i] = code_of<KW>(c, 0, dense);
+    idx[i] = i;
+  }
+}
+
+__global__ void bucket_pick_kernel(const uint64_t* __restrict__ sorted, uint32_t S, int parts,
+                                   uint64_t* __restrict__ split) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < parts - 1; j += gridDim.x * blockDim.x)
+    split[j] = sorted[(static_cast<uint64_t>(j) + 1) * S / parts];
+}
+
+// ------------------------------------------------------------------ coarse scatter
+
+struct CoarseParams {
+  const uint64_t* split;  // [B1-1]
+  int B1;
+  uint32_t capc;          // region capacity per coarse bucket
+  unsigned* fill;         // [B1] items per coarse bucket (may exceed capc: overflow)
+  uint32_t* idx_out;      // [B1][capc]
+  bool dense;
+  bool want_max;
+  unsigned long long* max_bits;
+};
+
+// Tiles of 8192 items: shared-memory histogram ranks, one global reservation
+// per (tile, bucket), then the index writes.
+template <int KW, class Src>
+__global__ void __launch_bounds__(kK1Threads, 2) bucket_coarse_kernel(Src src, uint32_t n, CoarseParams P) {
+  __shared__ uint64_t ss[kCoarseMax - 1];
+  __shared__ unsigned hist[kCoarseMax];
+  __shared__ unsigned base[kCoarseMax];
+  const int ns = P.B1 - 1;
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) ss[i] = P.split[i];
+  for (int i = threadIdx.x; i < P.B1; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  double mx = 0.0;
+  const uint64_t tile = static_cast<uint64_t>(blockDim.x) * kK1Items;
+  for (uint64_t t0 = blockIdx.x * tile; t0 < n; t0 += static_cast<uint64_t>(gridDim.x) * tile) {
+    uint32_t br[kK1Items];  // bucket << 16 | rank in tile
+#pragma unroll
+    for (int r = 0; r < kK1Items; ++r) {
+      const uint64_t p = t0 + static_cast<uint64_t>(r) * blockDim.x + threadIdx.x;
+      const bool valid = p < n;
+      int b = 0;
+      if (valid) {
+        if (P.want_max) {
+          uint64_t k[KW];
+          const c128 c = src.key_coeff(static_cast<uint32_t>(p), k);
+          const double a = wgd::hypot_ref(c.re, c.im);
+          if (mx < a) mx = a;  // std::max: a NaN never replaces the running max
+        }
+        uint64_t c[KW];
+        src.ckey(static_cast<uint32_t>(p), c);
+        b = upper_bound_u64(ss, ns, code_of<KW>(c, 0, P.dense));
+      }
+      const unsigned rk = warp_aggregated_add(hist, static_cast<unsigned>(b), valid);
+      br[r] = (static_cast<uint32_t>(b) << 16) | rk;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < P.B1; i += blockDim.x) {
+      const unsigned c = hist[i];
+      base[i] = c ? atomicAdd(P.fill + i, c) : 0u;
+      hist[i] = 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kK1Items; ++r) {
+      const uint64_t p = t0 + static_cast<uint64_t>(r) * blockDim.x + threadIdx.x;
+      if (p < n) {
+        const unsigned b = br[r] >> 16;
+        const unsigned pos = base[b] + (br[r] & 0xffffu);
+        if (pos < P.capc) P.idx_out[static_cast<size_t>(b) * P.capc + pos] = static_cast<uint32_t>(p);
+      }
+    }
+    __syncthreads();
+  }
+  if (P.want_max) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, mx, o);
+      if (mx < other) mx = other;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(P.max_bits, static_cast<unsigned long long>(__double_as_longlong(mx)));
+  }
+}
+
+// ------------------------------------------------------------------ plan
+
+__device__ __forceinline__ unsigned fine_target(unsigned n) {
+  const unsigned f = (n + kFineAvg - 1) / kFineAvg;
+  return f < 1 ? 1u : (f > kFineMax ? static_cast<unsigned>(kFineMax) : f);
+}
+
+// Fine bucket slots of a coarse bucket: the target count, a quarter more for
+// codes isolated on their own, and a few spare.
+__device__ __forceinline__ unsigned fine_slots(unsigned n) {
+  const unsigned t = fine_target(n);
+  return t + t / 4 + 8;
+}
+
+// Exclusive scan of one value per thread over the block (blockDim.x a multiple
+// of 32, at most 1024); the block total is returned through *total.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* warp_tmp, unsigned* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tmp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned w = lane < nw ? warp_tmp[lane] : 0u;
+    unsigned wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < nw) warp_tmp[lane] = wi - w;
+    if (lane == 31) warp_tmp[32] = wi;
+  }
+  __syncthreads();
+  const unsigned r = warp_tmp[warp] + incl - v;
+  *total = warp_tmp[32];
+  __syncthreads();
+  return r;
+}
+
+// One block of 1024 threads: coarse bucket sizes -> fine slot numbering, the
+// common prefix of every coarse bucket, and the cull threshold.
+__global__ void __launch_bounds__(1024) bucket_plan_kernel(const unsigned* __restrict__ fill, int B1, uint32_t capc,
+                                                           const uint64_t* __restrict__ split, int total, bool dense0,
+                                                           int thr_mode, double atol, double rtol, double thr_fixed,
+                                                           Control* ctl, uint32_t* __restrict__ fine_base,
+                                                           int* __restrict__ Lj) {
+  __shared__ unsigned warp_tmp[33];
+  unsigned carry = 0;
+  for (int j0 = 0; j0 < B1; j0 += blockDim.x) {
+    const int j = j0 + threadIdx.x;
+    unsigned slots = 0;
+    if (j < B1) {
+      const unsigned c = fill[j];
+      if (c > capc) atomicOr(&ctl->flags, kFlagCoarseFull);
+      slots = fine_slots(min(c, capc));
+      uint64_t lo, hi;
+      const int L = bucket_range(split, B1 - 1, j, lo, hi) ? child_prefix(0, dense0, total, lo, hi) : total;
+      Lj[j] = L | (dense_at(total, L) ? 0x10000 : 0);
+    }
+    unsigned tot;
+    const unsigned ex = block_exclusive_scan(slots, warp_tmp, &tot);
+    if (j < B1) fine_base[j] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) {
+    fine_base[B1] = carry;
+    ctl->fine_total = carry;
+    double thr = thr_fixed;
+    if (thr_mode == 1) {
+      const double mx = __longlong_as_double(static_cast<long long>(ctl->max_bits));
+      thr = wgd::add(atol, wgd::mul(rtol, mx));
+    } else if (thr_mode == 2) {
+      thr = atol;
+    }
+    ctl->thr = thr;
+  }
+}
+
+// ------------------------------------------------------------------ fine partition
+
+struct FineParams {
+  const unsigned* fill;
+  uint32_t capc;
+  int B1;
+  int total;
+  const uint32_t* fine_base;  // [B1+1]
+  const int* Lj;              // prefix | dense << 16
+  const uint32_t* idx_in;     // [B1][capc]
+  uint16_t* fid_tmp;          // [B1][capc] fine bucket of each item
+  uint64_t* rec_code;         // [B1][capc] in fine-bucket order
+  uint32_t* rec_idx;
+  uint32_t* fine_start;       // [G]
+  uint32_t* fine_count;       // [G] count | kExactBit | kPureBit
+  uint16_t* fine_L;           // [G] prefix of the bucket's codes
+  Control* ctl;
+};
+
+constexpr size_t kK2Smem = sizeof(uint64_t) * (kSample2 + kFineSlots) + sizeof(int) * kFineSlots +
+                           sizeof(unsigned) * kFineSlots;
+
+// Ascending bitonic sort of n (a power of two) words in shared memory.
+__device__ void smem_bitonic_u64(uint64_t* a, int n) {
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const uint64_t x = a[lo], y = a[hi];
+        const bool up = (lo & size) == 0;
+        if (up ? (y < x) : (x < y)) {
+          a[lo] = y;
+          a[hi] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int KW, class Src>
+__global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FineParams P) {
+  extern __shared__ __align__(16) unsigned char k2raw[];
+  uint64_t* samp = reinterpret_cast<uint64_t*>(k2raw);
+  uint64_t* fs = samp + kSample2;
+  int* fL = reinterpret_cast<int*>(fs + kFineSlots);
+  unsigned* cnt = reinterpret_cast<unsigned*>(fL + kFineSlots);
+  __shared__ unsigned s_job;
+  __shared__ int s_ns;
+  __shared__ unsigned warp_tmp[33];
+  const int total = P.total;
+  while (true) {
+    if (threadIdx.x == 0) s_job = atomicAdd(&P.ctl->k2_ticket, 1u);
+    __syncthreads();
+    const int j = static_cast<int>(s_job);
+    __syncthreads();
+    if (j >= P.B1) break;
+    const uint32_t n = min(P.fill[j], P.capc);
+    const size_t base = static_cast<size_t>(j) * P.capc;
+    const uint32_t g0 = P.fine_base[j];
+    const int slots = static_cast<int>(P.fine_base[j + 1] - g0);
+    const int target = static_cast<int>(fine_target(n));
+    const int Lp = P.Lj[j] & 0xffff;
+    const bool densep = (P.Lj[j] >> 16) & 1;
+    // random sample of codes relative to the coarse prefix, sorted
+    const int S2 = static_cast<int>(n < static_cast<uint32_t>(kSample2) ? n : static_cast<uint32_t>(kSample2));
+    int SP = 1;
+    while (SP < S2) SP <<= 1;
+    for (int t = threadIdx.x; t < SP; t += blockDim.x) {
+      uint64_t code = ~0ull;
+      if (t < S2) {
+        const uint32_t pos = S2 == static_cast<int>(n)
+                                 ? static_cast<uint32_t>(t)
+                                 : static_cast<uint32_t>(__umul64hi(mix64((static_cast<uint64_t>(j) << 32) | t), n));
+        uint64_t c[KW];
+        src.ckey(P.idx_in[base + pos], c);
+        code = code_of<KW>(c, Lp, densep);
+      }
+      samp[t] = code;
+    }
+    __syncthreads();
+    smem_bitonic_u64(samp, SP);
+    // Splitters, greedily: a bucket closes after the run of equal codes that
+    // brings it to its share of the sample; a code whose sample run stands for
+    // a quarter of kCap items or more (a heavily repeated key) gets a bucket of
+    // its own, [c, c + 1).
+    if (threadIdx.x == 0) {
+      const int share = max(1, S2 / target);
+      int ns = 0, acc = 0, i = 0;
+      while (i < S2 && ns < slots - 1) {
+        const uint64_t v = samp[i];
+        int r = 1;
+        while (i + r < S2 && samp[i + r] == v) ++r;
+        const bool heavy = r >= kHeavyRun && static_cast<uint64_t>(r) * n >= static_cast<uint64_t>(kCap / 4) * S2;
+        if (heavy && v != ~0ull && ns + 2 <= slots - 1) {
+          if (acc > 0 && (ns == 0 || fs[ns - 1] < v)) fs[ns++] = v;
+          fs[ns++] = v + 1;
+          acc = 0;
+        } else {
+          acc += r;
+          if (acc >= share && i + r < S2) {
+            fs[ns++] = samp[i + r];
+            acc = 0;
+          }
+        }
+        i += r;
+      }
+      s_ns = ns;
+    }
+    __syncthreads();
+    const int ns = s_ns;
+    for (int f = threadIdx.x; f < slots; f += blockDim.x) {
+      uint64_t lo, hi;
+      const int L = f <= ns && bucket_range(fs, ns, f, lo, hi) ? child_prefix(Lp, densep, total, lo, hi) : total;
+      fL[f] = L | (dense_at(total, L) ? 0x10000 : 0);
+      cnt[f] = 0;
+    }
+    __syncthreads();
+    // pass 1: fine bucket of every item
+    for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+      const uint32_t t = t0 + threadIdx.x;
+      const bool valid = t < n;
+      int f = 0;
+      if (valid) {
+        uint64_t c[KW];
+        src.ckey(P.idx_in[base + t], c);
+        f = upper_bound_u64(fs, ns, code_of<KW>(c, Lp, densep));
+        P.fid_tmp[base + t] = static_cast<uint16_t>(f);
+      }
+      warp_aggregated_add(cnt, static_cast<unsigned>(f), valid);
+    }
+    __syncthreads();
+    // fine bucket offsets (slots <= 1024: one or two rounds of the block scan)
+    unsigned carry = 0;
+    for (int f0 = 0; f0 < slots; f0 += blockDim.x) {
+      const int f = f0 + threadIdx.x;
+      const unsigned c = f < slots ? cnt[f] : 0u;
+      unsigned tot;
+      const unsigned ex = block_exclusive_scan(c, warp_tmp, &tot);
+      if (f < slots) {
+        const unsigned off = carry + ex;
+        const bool exact = (fL[f] >> 16) & 1;
+        const bool pure = exact && (fL[f] & 0xffff) == total;  // every key of the bucket is equal
+        P.fine_start[g0 + f] = static_cast<uint32_t>(base + off);
+        P.fine_count[g0 + f] = c | (exact ? kExactBit : 0u) | (pure ? kPureBit : 0u);
+        P.fine_L[g0 + f] = static_cast<uint16_t>(fL[f] & 0xffff);
+        cnt[f] = off;
+      }
+      carry += tot;
+    }
+    __syncthreads();
+    // pass 2: (code relative to the fine prefix, index) into fine-bucket order
+    for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+      const uint32_t t = t0 + threadIdx.x;
+      const bool valid = t < n;
+      const int f = valid ? P.fid_tmp[base + t] : 0;
+      const unsigned pos = warp_aggregated_add(cnt, static_cast<unsigned>(f), valid);
+      if (valid) {
+        const uint32_t p = P.idx_in[base + t];
+        uint64_t c[KW];
+        src.ckey(p, c);
+        const int Lf = fL[f];
+        P.rec_code[base + pos] = code_of<KW>(c, Lf & 0xffff, (Lf >> 16) & 1);
+        P.rec_idx[base + pos] = p;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ final
+
+struct FinalParams {
+  const uint32_t* fine_start;
+  const uint32_t* fine_count;
+  const uint16_t* fine_L;
+  const uint64_t* rec_code;
+  const uint32_t* rec_idx;
+  unsigned long long* state;  // look-back: flag | value per fine bucket
+  Control* ctl;
+  uint64_t* out_x;
+  uint64_t* out_z;
+  double* out_c;
+  size_t out_cap;  // terms the outputs hold
+};
+
+struct FinalSmem {
+  uint64_t code[kPadded];
+  uint32_t idx[kPadded];
+  uint32_t head[kWords];
+  uint32_t keep[kWords];
+  uint32_t wpre[kWords];
+  uint32_t runs[kMaxRuns];  // start << 16 | end of tie runs
+  unsigned n_runs;
+  unsigned warp_sum[kK3Threads / 32];
+  unsigned job;
+  unsigned kept;
+  unsigned long long excl;
+};
+
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ bool rec_less(uint64_t ca, uint32_t ia, uint64_t cb, uint32_t ib) {
+  return ca < cb || (ca == cb && ia < ib);
+}
+
+__device__ __forceinline__ bool bit_at(const uint32_t* m, int i) { return (m[i >> 5] >> (i & 31)) & 1u; }
+
+// First set bit after position i, or n.
+__device__ __forceinline__ int next_set(const uint32_t* m, int i, int n) {
+  const int p = i + 1;
+  if (p >= n) return n;
+  int w = p >> 5;
+  uint32_t v = m[w] & (~0u << (p & 31));
+  const int nw = (n + 31) >> 5;
+  while (!v) {
+    if (++w >= nw) return n;
+    v = m[w];
+  }
+  return min(n, (w << 5) + __ffs(v) - 1);
+}
+
+__device__ __forceinline__ void reg_sort16(uint64_t (&c)[kIPT], uint32_t (&x)[kIPT]) {
+#pragma unroll
+  for (int k = 2; k <= kIPT; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < kIPT; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const bool sw = up ? rec_less(c[l], x[l], c[i], x[i]) : rec_less(c[i], x[i], c[l], x[l]);
+          const uint64_t ci = c[i], cl = c[l];
+          const uint32_t xi = x[i], xl = x[l];
+          c[i] = sw ? cl : ci;
+          c[l] = sw ? ci : cl;
+          x[i] = sw ? xl : xi;
+          x[l] = sw ? xi : xl;
+        }
+      }
+    }
+  }
+}
+
+// Sorts the first n_pad (a power of two, >= kIPT) records by (code, idx):
+// sorted runs of 16 per thread in registers, then merge-path merges.
+__device__ void block_merge_sort(FinalSmem& S, int n_pad) {
+  const int active = n_pad / kIPT;
+  const int t = threadIdx.x;
+  uint64_t c[kIPT];
+  uint32_t x[kIPT];
+  if (t < active) {
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) {
+      c[k] = S.code[pidx(t * kIPT + k)];
+      x[k] = S.idx[pidx(t * kIPT + k)];
+    }
+    reg_sort16(c, x);
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) {
+      S.code[pidx(t * kIPT + k)] = c[k];
+      S.idx[pidx(t * kIPT + k)] = x[k];
+    }
+  }
+  __syncthreads();
+  for (int R = kIPT; R < n_pad; R <<= 1) {
+    if (t < active) {
+      const int pos = t * kIPT;
+      const int base = pos & ~(2 * R - 1);
+      const int diag = pos - base;
+      int lo = max(0, diag - R), hi = min(diag, R);
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const int ai = pidx(base + mid), bi = pidx(base + R + diag - 1 - mid);
+        if (!rec_less(S.code[bi], S.idx[bi], S.code[ai], S.idx[ai])) lo = mid + 1;
+        else hi = mid;
+      }
+      int ia = base + lo, ib = base + R + (diag - lo);
+      const int ea = base + R, eb = base + 2 * R;
+      uint64_t ca = ia < ea ? S.code[pidx(ia)] : 0ull;
+      uint32_t xa = ia < ea ? S.idx[pidx(ia)] : 0u;
+      uint64_t cb = ib < eb ? S.code[pidx(ib)] : 0ull;
+      uint32_t xb = ib < eb ? S.idx[pidx(ib)] : 0u;
+#pragma unroll
+      for (int k = 0; k < kIPT; ++k) {
+        const bool take_a = ia < ea && (ib >= eb || !rec_less(cb, xb, ca, xa));
+        c[k] = take_a ? ca : cb;
+        x[k] = take_a ? xa : xb;
+        if (take_a) {
+          ++ia;
+          if (ia < ea) {
+            ca = S.code[pidx(ia)];
+            xa = S.idx[pidx(ia)];
+          }
+        } else {
+          ++ib;
+          if (ib < eb) {
+            cb = S.code[pidx(ib)];
+            xb = S.idx[pidx(ib)];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (t < active) {
+#pragma unroll
+      for (int k = 0; k < kIPT; ++k) {
+        S.code[pidx(t * kIPT + k)] = c[k];
+        S.idx[pidx(t * kIPT + k)] = x[k];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Insertion sort of sorted positions [i, e) by (code, idx); the run is short,
+// or already ordered (then each insertion stops at once).
+__device__ void insertion_sort(FinalSmem& S, int i, int e) {
+  for (int q = i + 1; q < e; ++q) {
+    const uint64_t cq = S.code[pidx(q)];
+    const uint32_t xq = S.idx[pidx(q)];
+    int r = q;
+    while (r > i && rec_less(cq, xq, S.code[pidx(r - 1)], S.idx[pidx(r - 1)])) {
+      S.code[pidx(r)] = S.code[pidx(r - 1)];
+      S.idx[pidx(r)] = S.idx[pidx(r - 1)];
+      --r;
+    }
+    S.code[pidx(r)] = cq;
+    S.idx[pidx(r)] = xq;
+  }
+}
+
+// Positions [i, e) hold one tie of 16-digit codes: keys with more than 16 set
+// bits after the prefix may still differ.  Reordered by (key, index) -- the
+// distinct keys (at most kDistinct) are sorted, then each key's items are
+// emitted in index order -- with a segment head where the key changes.  The
+// code slots of the range are free by now and carry the indices on the way.
+template <int KW, class Src>
+__device__ void resolve_mixed(const Src& src, FinalSmem& S, int i, int e, unsigned* flags) {
+  uint64_t D[kDistinct][KW];
+  int nd = 0;
+  for (int m = i; m < e; ++m) {
+    uint64_t k[KW];
+    src.key(S.idx[pidx(m)], k);
+    bool seen = false;
+    for (int d = 0; d < nd && !seen; ++d) {
+      bool eq = true;
+      for (int w = 0; w < KW; ++w) eq = eq && D[d][w] == k[w];
+      seen = eq;
+    }
+    if (seen) continue;
+    if (nd == kDistinct) {
+      atomicOr(flags, kFlagDistinct);
+      return;
+    }
+    for (int w = 0; w < KW; ++w) D[nd][w] = k[w];
+    ++nd;
+  }
+  if (nd == 1) return;
+  for (int q = 1; q < nd; ++q) {
+    uint64_t kq[KW];
+    for (int w = 0; w < KW; ++w) kq[w] = D[q][w];
+    int r = q;
+    while (r > 0) {
+      uint64_t kp[KW];
+      for (int w = 0; w < KW; ++w) kp[w] = D[r - 1][w];
+      if (!kless<KW>(kq, kp)) break;
+      for (int w = 0; w < KW; ++w) D[r][w] = kp[w];
+      --r;
+    }
+    for (int w = 0; w < KW; ++w) D[r][w] = kq[w];
+  }
+  int o = i;
+  for (int d = 0; d < nd; ++d) {
+    if (d > 0) atomicOr(&S.head[o >> 5], 1u << (o & 31));
+    uint64_t kd[KW];
+    for (int w = 0; w < KW; ++w) kd[w] = D[d][w];
+    for (int m = i; m < e; ++m) {
+      const uint32_t id = S.idx[pidx(m)];
+      uint64_t k[KW];
+      src.key(id, k);
+      if (keq<KW>(k, kd)) S.code[pidx(o++)] = id;
+    }
+  }
+  for (int m = i; m < e; ++m) S.idx[pidx(m)] = static_cast<uint32_t>(S.code[pidx(m)]);
+}
+
+// A run [i, e) of equal 8-digit position codes: the items take their next
+// eight digits as code and are reordered by (code, index); a head goes where
+// that code changes, and ties of all 16 digits with a 16th digit (the key may
+// have more set bits) are checked key by key.
+template <int KW, class Src>
+__device__ void resolve_tie(const Src& src, FinalSmem& S, int i, int e, int L, unsigned* flags) {
+  for (int m = i; m < e; ++m) {
+    uint64_t c[KW];
+    src.ckey(S.idx[pidx(m)], c);
+    S.code[pidx(m)] = position_code<KW>(c, L, 8);
+  }
+  insertion_sort(S, i, e);
+  int s = i;
+  while (s < e) {
+    const uint64_t cs = S.code[pidx(s)];
+    int t = s + 1;
+    while (t < e && S.code[pidx(t)] == cs) ++t;
+    if (s > i) atomicOr(&S.head[s >> 5], 1u << (s & 31));
+    if (t - s > 1 && (cs & 0xffu) != 0) resolve_mixed<KW>(src, S, s, t, flags);
+    s = t;
+  }
+}
+
+// Left-to-right sum of the coefficients of sorted positions [i, e); flags any
+// coefficient of infinite magnitude.
+template <int KW, class Src>
+__device__ __forceinline__ c128 segment_sum(const Src& src, const FinalSmem& S, int i, int e, bool& inf) {
+  c128 acc{0.0, 0.0};
+  for (int m = i; m < e; ++m) {
+    uint64_t k[KW];
+    const c128 c = src.key_coeff(S.idx[pidx(m)], k);
+    if (!(fabs(c.re) <= 0x1p1022 && fabs(c.im) <= 0x1p1022) && isinf(wgd::hypot_ref(c.re, c.im))) inf = true;
+    acc = wgd::cadd(acc, c);
+  }
+  return acc;
+}
+
+static_assert(kK3Threads == 256, "radix_sort_u32 maps one thread per digit");
+static_assert(sizeof(unsigned) * (256 + (kK3Threads / 32) * 256 + 2) <= sizeof(uint64_t) * kPadded,
+              "radix_sort_u32 scratch must fit in the code area");
+
+// Stable LSD radix sort (8-bit digits) of n indices in global memory by one
+// block, ping-ponging between a and tmp; digits on which all indices agree are
+// skipped.  Returns the array that holds the sorted indices.  Scratch lives in
+// the (unused) code area of the shared-memory tile.
+__device__ const uint32_t* radix_sort_u32(FinalSmem& S, uint32_t* a, uint32_t* tmp, int n) {
+  unsigned* hist = reinterpret_cast<unsigned*>(S.code);           // [256]
+  unsigned* wcnt = hist + 256;                                      // [8][256]
+  unsigned* red = wcnt + (kK3Threads / 32) * 256;                   // [2]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < 2) red[tid] = tid == 0 ? 0u : ~0u;
+  __syncthreads();
+  unsigned o = 0, d = ~0u;
+  for (int i = tid; i < n; i += kK3Threads) {
+    o |= a[i];
+    d &= a[i];
+  }
+  atomicOr(&red[0], o);
+  atomicAnd(&red[1], d);
+  __syncthreads();
+  const unsigned vary = red[0] ^ red[1];
+  uint32_t* src = a;
+  uint32_t* dst = tmp;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int sh = 0; sh < 32; sh += 8) {
+    if (((vary >> sh) & 0xffu) == 0) continue;
+    hist[tid] = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += kK3Threads) atomicAdd(&hist[(src[i] >> sh) & 0xffu], 1u);
+    __syncthreads();
+    if (warp == 0) {
+      // exclusive scan of 256 counts, 8 per lane
+      unsigned v[8], t = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        v[q] = hist[lane * 8 + q];
+        t += v[q];
+      }
+      unsigned incl = t;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+      }
+      unsigned run = incl - t;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        hist[lane * 8 + q] = run;
+        run += v[q];
+      }
+    }
+    __syncthreads();
+    for (int i0 = 0; i0 < n; i0 += kK3Threads) {
+      const int i = i0 + tid;
+      const bool valid = i < n;
+      const uint32_t val = valid ? src[i] : 0u;
+      const unsigned dg = valid ? (val >> sh) & 0xffu : 0x100u;
+      for (int e = tid; e < (kK3Threads / 32) * 256; e += kK3Threads) wcnt[e] = 0;
+      __syncthreads();
+      const unsigned peers = __match_any_sync(0xffffffffu, dg);
+      const unsigned rank = __popc(peers & lt);
+      if (valid && rank == 0) wcnt[warp * 256 + dg] = __popc(peers);
+      __syncthreads();
+      {
+        unsigned run = hist[tid];
+        for (int w = 0; w < kK3Threads / 32; ++w) {
+          const unsigned c = wcnt[w * 256 + tid];
+          wcnt[w * 256 + tid] = run;
+          run += c;
+        }
+        hist[tid] = run;
+      }
+      __syncthreads();
+      if (valid) dst[wcnt[warp * 256 + dg] + rank] = val;
+      __syncthreads();
+    }
+    uint32_t* t2 = src;
+    src = dst;
+    dst = t2;
+  }
+  __threadfence_block();
+  __syncthreads();
+  return src;
+}
+
+template <int KW, class Src>
+__global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, FinalParams P) {
+  extern __shared__ __align__(16) unsigned char k3raw[];
+  FinalSmem& S = *reinterpret_cast<FinalSmem*>(k3raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned G = P.ctl->fine_total;
+  const double thr = P.ctl->thr;
+  bool inf = false;
+  while (true) {
+    if (tid == 0) S.job = atomicAdd(&P.ctl->k3_ticket, 1u);
+    __syncthreads();
+    const unsigned g = S.job;
+    __syncthreads();
+    if (g >= G) break;
+    const uint32_t start = P.fine_start[g];
+    const uint32_t cw = P.fine_count[g];
+    const int n = static_cast<int>(cw & kCountMask);
+    const bool exact = (cw & kExactBit) != 0;
+    const bool pure = (cw & kPureBit) != 0;
+    const bool fits = n <= kCap;
+    unsigned count = 0;
+    if (tid == 0 && n > 0) {
+      if (!fits && !pure) atomicOr(&P.ctl->flags, kFlagFineFull);
+      atomicMax(&P.ctl->max_fine, static_cast<unsigned>(n));
+    }
+    c128 big_sum{0.0, 0.0};
+    uint32_t big_first = 0;
+    if (!fits && pure) {
+      // one key, more items than shared memory holds: sort the indices in
+      // global memory, then one thread sums them in index order
+      uint32_t* a = const_cast<uint32_t*>(P.rec_idx) + start;
+      uint32_t* tmp = reinterpret_cast<uint32_t*>(const_cast<uint64_t*>(P.rec_code) + start);
+      const uint32_t* sorted = radix_sort_u32(S, a, tmp, n);
+      if (tid == 0) {
+        for (int m = 0; m < n; ++m) {
+          uint64_t k[KW];
+          const c128 c = src.key_coeff(sorted[m], k);
+          if (!(fabs(c.re) <= 0x1p1022 && fabs(c.im) <= 0x1p1022) && isinf(wgd::hypot_ref(c.re, c.im))) inf = true;
+          big_sum = wgd::cadd(big_sum, c);
+        }
+        big_first = sorted[0];
+        S.kept = wgd::hypot_ref(big_sum.re, big_sum.im) > thr ? 1u : 0u;
+      }
+      __syncthreads();
+      count = S.kept;
+    }
+    if (fits && n > 0) {
+      int n_pad = kIPT;
+      while (n_pad < n) n_pad <<= 1;
+      for (int i = tid; i < n_pad; i += kK3Threads) {
+        S.code[pidx(i)] = i < n ? P.rec_code[start + i] : ~0ull;
+        S.idx[pidx(i)] = i < n ? P.rec_idx[start + i] : ~0u;
+      }
+      for (int w = tid; w < kWords; w += kK3Threads) {
+        S.head[w] = 0;
+        S.keep[w] = 0;
+      }
+      if (tid == 0) S.n_runs = 0;
+      __syncthreads();
+      block_merge_sort(S, n_pad);
+      // segment heads where the code changes
+      for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
+        const int i = i0 + lane;
+        const bool h = i < n && (i == 0 || S.code[pidx(i)] != S.code[pidx(i - 1)]);
+        const uint32_t b = __ballot_sync(0xffffffffu, h);
+        if (lane == 0) S.head[i0 >> 5] = b;
+      }
+      if (!exact) {
+        // runs of equal position code, listed by the thread at the run's first
+        // position, then resolved once every thread is done reading codes
+        for (int i = tid; i + 1 < n; i += kK3Threads) {
+          const uint64_t ci = S.code[pidx(i)];
+          // a code with an empty eighth digit holds every set bit: one key
+          if ((ci & 0xffu) == 0 || (i > 0 && S.code[pidx(i - 1)] == ci) || S.code[pidx(i + 1)] != ci) continue;
+          int e = i + 2;
+          while (e < n && S.code[pidx(e)] == ci) ++e;
+          const unsigned q = atomicAdd(&S.n_runs, 1u);
+          S.runs[q] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(e);
+        }
+        __syncthreads();
+        const int L = P.fine_L[g];
+        const int nr = static_cast<int>(S.n_runs);
+        for (int q = tid; q < nr; q += kK3Threads)
+          resolve_tie<KW>(src, S, static_cast<int>(S.runs[q] >> 16), static_cast<int>(S.runs[q] & 0xffffu), L,
+                          &P.ctl->flags);
+      }
+      __syncthreads();
+      // segment sums and the cull
+      for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
+        const int i = i0 + lane;
+        bool kp = false;
+        if (i < n && bit_at(S.head, i)) {
+          const c128 s = segment_sum<KW>(src, S, i, next_set(S.head, i, n), inf);
+          kp = wgd::hypot_ref(s.re, s.im) > thr;
+        }
+        const uint32_t b = __ballot_sync(0xffffffffu, kp);
+        if (lane == 0) S.keep[i0 >> 5] = b;
+      }
+      __syncthreads();
+      unsigned c = 0;
+      for (int w = tid; w < (n + 31) / 32; w += kK3Threads) c += __popc(S.keep[w]);
+#pragma unroll
+      for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == 0) S.warp_sum[warp] = c;
+      __syncthreads();
+      if (tid == 0) {
+        unsigned tsum = 0;
+        for (int w = 0; w < kK3Threads / 32; ++w) tsum += S.warp_sum[w];
+        S.kept = tsum;
+      }
+      __syncthreads();
+      count = S.kept;
+    }
+    // decoupled look-back over the preceding fine buckets (bounded polling)
+    if (tid == 0) {
+      unsigned long long excl = 0;
+      if (g > 0) {
+        atomicExch(P.state + g, kStAgg | count);
+        long k = static_cast<long>(g) - 1;
+        unsigned polls = 0;
+        while (k >= 0) {
+          const unsigned long long v = *reinterpret_cast<volatile unsigned long long*>(P.state + k);
+          const unsigned long long fl = v & ~kStValue;
+          if (fl == 0) {
+            if (++polls > kSpinLimit) {
+              atomicOr(&P.ctl->flags, kFlagTimeout);
+              break;
+            }
+            __nanosleep(100);
+            continue;
+          }
+          excl += v & kStValue;
+          if (fl == kStIncl) break;
+          --k;
+        }
+      }
+      atomicExch(P.state + g, kStIncl | (excl + count));
+      if (g == G - 1) P.ctl->survivors = excl + count;
+      S.excl = excl;
+    }
+    __syncthreads();
+    if (!fits && pure && count > 0 && tid == 0) {
+      const size_t o = S.excl;
+      if (o >= P.out_cap) {
+        atomicOr(&P.ctl->flags, kFlagOverrun);
+      } else {
+        uint64_t k[KW];
+        src.key(big_first, k);
+#pragma unroll
+        for (int w = 0; w < KW / 2; ++w) {
+          P.out_x[o * (KW / 2) + w] = k[2 * w];
+          P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
+        }
+        P.out_c[2 * o] = big_sum.re;
+        P.out_c[2 * o + 1] = big_sum.im;
+      }
+    }
+    if (fits && count > 0) {
+      const int nw = (n + 31) / 32;
+      if (warp == 0) {
+        // exclusive prefix of survivors per bitmask word (at most 4 words per lane)
+        unsigned v[4], s = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int w = lane * 4 + q;
+          v[q] = w < nw ? __popc(S.keep[w]) : 0u;
+          s += v[q];
+        }
+        unsigned incl = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        unsigned run = incl - s;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int w = lane * 4 + q;
+          if (w < nw) S.wpre[w] = run;
+          run += v[q];
+        }
+      }
+      __syncthreads();
+      const unsigned long long excl = S.excl;
+      for (int i = tid; i < n; i += kK3Threads) {
+        if (!bit_at(S.keep, i)) continue;
+        const size_t o = excl + S.wpre[i >> 5] + __popc(S.keep[i >> 5] & ((1u << (i & 31)) - 1u));
+        if (o >= P.out_cap) {
+          atomicOr(&P.ctl->flags, kFlagOverrun);
+          continue;
+        }
+        uint64_t k[KW];
+        src.key(S.idx[pidx(i)], k);
+        bool unused = false;
+        const c128 s = segment_sum<KW>(src, S, i, next_set(S.head, i, n), unused);
+#pragma unroll
+        for (int w = 0; w < KW / 2; ++w) {
+          P.out_x[o * (KW / 2) + w] = k[2 * w];
+          P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
+        }
+        P.out_c[2 * o] = s.re;
+        P.out_c[2 * o + 1] = s.im;
+      }
+    }
+    __syncthreads();
+  }
+  if (inf) atomicOr(&P.ctl->inf_seen, 1u);
+}
+
+// ------------------------------------------------------------------ host side
+
+std::atomic<int> g_sort_algorithm{WG_SORT_AUTO};
+thread_local int t_last_sort = 0;
+
+struct ThrSpec {
+  int mode;  // 0 fixed, 1 atol + rtol * max|c|, 2 atol (an infinite |c| empties the result)
+  double atol, rtol, fixed;
+};
+
+struct Outs {
+  uint64_t** x;
+  uint64_t** z;
+  double** c;
+  size_t* n;
+};
+
+template <class K>
+void set_smem(K kernel, size_t bytes) {
+  wg::check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
+                 "set bucket kernel shared memory");
+}
+
+template <int KW, class Src>
+bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec& thr, const Outs& out,
+                cudaStream_t s) {
+  const int W = KW / 2;
+  const bool dense0 = total <= 64;
+  int B1 = 2;
+  while (B1 < kCoarseMax && (static_cast<uint64_t>(B1) << kCoarseLog) < n) B1 <<= 1;
+  const uint64_t avg = (static_cast<uint64_t>(n) + B1 - 1) / B1;
+  const uint64_t capc64 = 2 * avg + 8192;
+  if (capc64 > static_cast<uint64_t>(kFineMax) * kFineAvg) return false;  // fine buckets would overflow
+  const uint32_t capc = static_cast<uint32_t>(capc64);
+  const size_t region = static_cast<size_t>(B1) * capc;
+  // fine slots: sum over coarse buckets of t + t/4 + 8 with t <= n_j/kFineAvg + 1
+  const size_t Gmax = (static_cast<size_t>(n) / kFineAvg + B1) * 5 / 4 + static_cast<size_t>(B1) * 9 + 1;
+  const auto& props = wg::device_props(device);
+
+  wg::Scratch ctl(sizeof(Control), s);
+  wg::check_cuda(cudaMemsetAsync(ctl.get(), 0, sizeof(Control), s), "clear bucket control");
+  Control* dctl = ctl.as<Control>();
+
+  // coarse splitters from a sorted sample of codes
+  const uint32_t S1 = static_cast<uint32_t>(std::min<uint64_t>(n, static_cast<uint64_t>(kCoarseSample) * B1));
+  wg::Scratch split(sizeof(uint64_t) * B1, s);
+  {
+    wg::Scratch skeys(sizeof(uint64_t) * S1, s), sidx(sizeof(uint32_t) * S1, s);
+    WG_TIMED("bucket_sample_kernel", s,
+      bucket_sample_kernel<KW><<<wg::grid_for(S1, 256, device, 4), 256, 0, s>>>(src, n, S1, dense0,
+                                                                                 skeys.as<uint64_t>(),
+                                                                                 sidx.as<uint32_t>()));
+    wg::check_launch("launch bucket sample");
+    wg::radix_sort_keys(device, S1, 1, skeys, sidx, s);
+    WG_TIMED("bucket_pick_kernel", s,
+      bucket_pick_kernel<<<(B1 + 255) / 256, 256, 0, s>>>(skeys.as<uint64_t>(), S1, B1, split.as<uint64_t>()));
+    wg::check_launch("launch bucket splitters");
+  }
+
+  // coarse scatter
+  wg::Scratch fill(sizeof(unsigned) * B1, s), idx1(sizeof(uint32_t) * region, s);
+  wg::check_cuda(cudaMemsetAsync(fill.get(), 0, sizeof(unsigned) * B1, s), "clear coarse fill");
+  {
+    const CoarseParams cp{split.as<uint64_t>(), B1, capc, fill.as<unsigned>(), idx1.as<uint32_t>(), dense0,
+                          thr.mode == 1, &dctl->max_bits};
+    const unsigned grid = wg::grid_for(n, kK1Threads * kK1Items, device, 2);
+    WG_TIMED("bucket_coarse_kernel", s, bucket_coarse_kernel<KW><<<grid, kK1Threads, 0, s>>>(src, n, cp));
+    wg::check_launch("launch coarse scatter");
+  }
+  wg::Scratch fine_base(sizeof(uint32_t) * (B1 + 1), s), Lj(sizeof(int) * B1, s);
+  WG_TIMED("bucket_plan_kernel", s,
+    bucket_plan_kernel<<<1, 1024, 0, s>>>(fill.as<unsigned>(), B1, capc, split.as<uint64_t>(), total, dense0,
+                                          thr.mode, thr.atol, thr.rtol, thr.fixed, dctl, fine_base.as<uint32_t>(),
+                                          Lj.as<int>()));
+  wg::check_launch("launch bucket plan");
+
+  // fine partition
+  wg::Scratch rec_code(sizeof(uint64_t) * region, s), rec_idx(sizeof(uint32_t) * region, s);
+  wg::Scratch fine_start(sizeof(uint32_t) * Gmax, s), fine_count(sizeof(uint32_t) * Gmax, s),
+      fine_L(sizeof(uint16_t) * Gmax, s);
+  {
+    wg::Scratch fid_tmp(sizeof(uint16_t) * region, s);
+    const FineParams fp{fill.as<unsigned>(), capc, B1, total, fine_base.as<uint32_t>(), Lj.as<int>(),
+                        idx1.as<uint32_t>(), fid_tmp.as<uint16_t>(), rec_code.as<uint64_t>(), rec_idx.as<uint32_t>(),
+                        fine_start.as<uint32_t>(), fine_count.as<uint32_t>(), fine_L.as<uint16_t>(), dctl};
+    auto* k2 = bucket_fine_kernel<KW, Src>;
+    set_smem(k2, kK2Smem);
+    int per_sm = 0;
+    wg::check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2, kK2Threads, kK2Smem),
+                   "query fine occupancy");
+    const unsigned grid = static_cast<unsigned>(std::min<int>(B1, props.sm_count * std::max(1, per_sm)));
+    WG_TIMED("bucket_fine_kernel", s, k2<<<grid, kK2Threads, kK2Smem, s>>>(src, fp));
+    wg::check_launch("launch fine partition");
+  }
+  idx1.release();
+
+  // final: outputs at capacity n (shrunk below when far fewer survive)
+  const size_t nn = n;
+  wg::Scratch ox(sizeof(uint64_t) * W * nn, s), oz(sizeof(uint64_t) * W * nn, s), oc(sizeof(double) * 2 * nn, s);
+  wg::Scratch state(sizeof(unsigned long long) * Gmax, s);
+  wg::check_cuda(cudaMemsetAsync(state.get(), 0, sizeof(unsigned long long) * Gmax, s), "clear look-back state");
+  {
+    const FinalParams fp{fine_start.as<uint32_t>(), fine_count.as<uint32_t>(), fine_L.as<uint16_t>(),
+                         rec_code.as<uint64_t>(), rec_idx.as<uint32_t>(), state.as<unsigned long long>(), dctl,
+                         ox.as<uint64_t>(), oz.as<uint64_t>(), oc.as<double>(), nn};
+    auto* k3 = bucket_final_kernel<KW, Src>;
+    set_smem(k3, sizeof(FinalSmem));
+    int per_sm = 0;
+    wg::check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3, kK3Threads, sizeof(FinalSmem)),
+                   "query final occupancy");
+    const unsigned grid = static_cast<unsigned>(props.sm_count * std::max(1, per_sm));
+    WG_TIMED("bucket_final_kernel", s, k3<<<grid, kK3Threads, sizeof(FinalSmem), s>>>(src, fp));
+    wg::check_launch("launch bucket final");
+  }
+  Control h{};
+  wg::check_cuda(cudaMemcpyAsync(&h, dctl, sizeof(Control), cudaMemcpyDeviceToHost, s), "read bucket control");
+  wg::check_cuda(cudaStreamSynchronize(s), "synchronize bucket sort");
+  if (std::getenv("WG_BUCKET_TRACE"))
+    std::fprintf(stderr, "bucket: n=%u coarse=%d fine=%u max_fine=%u flags=0x%x survivors=%llu\n", n, B1,
+                 h.fine_total, h.max_fine, h.flags, h.survivors);
+  if (h.flags & kFlagTimeout)
+    throw wg::Error(WG_ERR_TIMEOUT, "bucketed simplify: a fine bucket waited too long for its predecessors");
+  if (h.flags & kFlagOverrun) throw wg::Error(WG_ERR_CUDA, "bucketed simplify: output rank beyond capacity");
+  if (h.flags & kFallbackMask) return false;
+  size_t U = static_cast<size_t>(h.survivors);
+  if (thr.mode == 2 && h.inf_seen) U = 0;  // atol + 0 * inf is NaN: nothing survives
+  *out.n = U;
+  *out.x = *out.z = nullptr;
+  *out.c = nullptr;
+  if (U == 0) return true;
+  if (U < nn / 4 * 3) {
+    wg::Scratch sx(sizeof(uint64_t) * W * U, s), sz(sizeof(uint64_t) * W * U, s), sc(sizeof(double) * 2 * U, s);
+    wg::check_cuda(cudaMemcpyAsync(sx.get(), ox.get(), sizeof(uint64_t) * W * U, cudaMemcpyDeviceToDevice, s),
+                   "shrink outputs");
+    wg::check_cuda(cudaMemcpyAsync(sz.get(), oz.get(), sizeof(uint64_t) * W * U, cudaMemcpyDeviceToDevice, s),
+                   "shrink outputs");
+    wg::check_cuda(cudaMemcpyAsync(sc.get(), oc.get(), sizeof(double) * 2 * U, cudaMemcpyDeviceToDevice, s),
+                   "shrink outputs");
+    std::swap(ox, sx);
+    std::swap(oz, sz);
+    std::swap(oc, sc);
+  }
+  wg::check_cuda(cudaStreamSynchronize(s), "synchronize bucket outputs");
+  *out.x = static_cast<uint64_t*>(ox.detach());
+  *out.z = static_cast<uint64_t*>(oz.detach());
+  *out.c = static_cast<double*>(oc.detach());
+  return true;
+}
+
+// Packs terms to AoS keys (+ y) and ORs their words into sig (device).
+void pack(const uint64_t* x, const uint64_t* z, size_t T, int W, wg::Scratch& keys, wg::Scratch* y,
+          unsigned long long* sig, int device, cudaStream_t s) {
+  keys.reset(sizeof(uint64_t) * 2 * W * std::max<size_t>(T, 1), s);
+  if (y) y->reset(std::max<size_t>(T, 1), s);
+  WG_TIMED("bucket_pack_kernel", s,
+    bucket_pack_kernel<<<wg::grid_for(T, 256, device, 4), 256, 0, s>>>(x, z, T, W, keys.as<uint64_t>(),
+                                                                        y ? y->as<uint8_t>() : nullptr, sig));
+  wg::check_launch("launch bucket pack");
+}
+
+void compress(const wg::Scratch& keys, size_t T, int KW, const SigWords& sig, wg::Scratch& out, int device,
+              cudaStream_t s) {
+  out.reset(sizeof(uint64_t) * KW * std::max<size_t>(T, 1), s);
+  WG_TIMED("bucket_compress_kernel", s,
+    bucket_compress_kernel<<<wg::grid_for(T, 256, device, 4), 256, 0, s>>>(keys.as<uint64_t>(), T, KW, sig,
+                                                                            out.as<uint64_t>()));
+  wg::check_launch("launch bucket compress");
+}
+
+// Significant bits of the packed keys (host copy) and their count.
+int read_sig(const wg::Scratch& sig, int KW, SigWords& out, cudaStream_t s) {
+  unsigned long long h[4] = {0, 0, 0, 0};
+  wg::check_cuda(cudaMemcpyAsync(h, sig.get(), sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, s),
+                 "read significant bits");
+  wg::check_cuda(cudaStreamSynchronize(s), "read significant bits");
+  int total = 0;
+  for (int w = 0; w < 4; ++w) {
+    out.w[w] = w < KW ? h[w] : 0ull;
+    total += __builtin_popcountll(out.w[w]);
+  }
+  return total;
+}
+
+}  // namespace
+
+namespace wg {
+
+int sort_algorithm() { return g_sort_algorithm.load(std::memory_order_relaxed); }
+void note_sort(int algo) { t_last_sort = algo; }
+
+bool bucket_products(int device, int W, const uint64_t* lx, const uint64_t* lz, const double* lc, size_t n_l,
+                     const uint64_t* rx, const uint64_t* rz, const double* rc, size_t n_r, int thr_mode, double atol,
+                     double rtol, double thr_fixed, uint64_t** ox, uint64_t** oz, double** oc, size_t* U,
+                     cudaStream_t s) {
+  if (W < 1 || W > 2 || n_l == 0 || n_r == 0 || n_l > 0xffffffffull || n_r > 0xffffffffull) return false;
+  const size_t P = n_l * n_r;
+  if (P > 0xffffffffull) return false;
+  const int KW = 2 * W;
+  Scratch sig(sizeof(unsigned long long) * 4, s);
+  check_cuda(cudaMemsetAsync(sig.get(), 0, sizeof(unsigned long long) * 4, s), "clear significant bits");
+  Scratch ak, bk, ay, by, ac2, bc2;
+  pack(lx, lz, n_l, W, ak, &ay, sig.as<unsigned long long>(), device, s);
+  pack(rx, rz, n_r, W, bk, &by, sig.as<unsigned long long>(), device, s);
+  SigWords sw{};
+  const int total = read_sig(sig, KW, sw, s);
+  if (total < 1 || total > 255) return false;
+  compress(ak, n_l, KW, sw, ac2, device, s);
+  compress(bk, n_r, KW, sw, bc2, device, s);
+  const ThrSpec thr{thr_mode, atol, rtol, thr_fixed};
+  const Outs out{ox, oz, oc, U};
+  const FastDiv fd{static_cast<uint32_t>(n_r), n_r > 1 ? ~0ull / n_r + 1 : 0ull};
+  if (W == 1) {
+    const ProdSrc<2> src{ak.as<uint64_t>(), bk.as<uint64_t>(), ac2.as<uint64_t>(), bc2.as<uint64_t>(),
+                         lc, rc, ay.as<uint8_t>(), by.as<uint8_t>(), fd};
+    return run_bucket<2>(device, src, static_cast<uint32_t>(P), total, thr, out, s);
+  }
+  const ProdSrc<4> src{ak.as<uint64_t>(), bk.as<uint64_t>(), ac2.as<uint64_t>(), bc2.as<uint64_t>(),
+                       lc, rc, ay.as<uint8_t>(), by.as<uint8_t>(), fd};
+  return run_bucket<4>(device, src, static_cast<uint32_t>(P), total, thr, out, s);
+}
+
+bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, const double* c, size_t n,
+                     int thr_mode, double atol, double rtol, uint64_t** ox, uint64_t** oz, double** oc, size_t* U,
+                     cudaStream_t s) {
+  if (W < 1 || W > 2 || n == 0 || n > 0xffffffffull) return false;
+  const int KW = 2 * W;
+  Scratch sig(sizeof(unsigned long long) * 4, s);
+  check_cuda(cudaMemsetAsync(sig.get(), 0, sizeof(unsigned long long) * 4, s), "clear significant bits");
+  Scratch tk, tc2;
+  pack(x, z, n, W, tk, nullptr, sig.as<unsigned long long>(), device, s);
+  SigWords sw{};
+  const int total = read_sig(sig, KW, sw, s);
+  if (total < 1 || total > 255) return false;
+  compress(tk, n, KW, sw, tc2, device, s);
+  const ThrSpec thr{thr_mode, atol, rtol, 0.0};
+  const Outs out{ox, oz, oc, U};
+  if (W == 1) {
+    const TermSrc<2> src{tk.as<uint64_t>(), tc2.as<uint64_t>(), c};
+    return run_bucket<2>(device, src, static_cast<uint32_t>(n), total, thr, out, s);
+  }
+  const TermSrc<4> src{tk.as<uint64_t>(), tc2.as<uint64_t>(), c};
+  return run_bucket<4>(device, src, static_cast<uint32_t>(n), total, thr, out, s);
+}
+
+}  // namespace wg
+
+extern "C" {
+
+int wg_set_sort_algorithm(int algo) {
+  return wg::guarded([&] {
+    if (algo != WG_SORT_AUTO && algo != WG_SORT_LSD && algo != WG_SORT_BUCKET)
+      wg::throw_invalid("sort algorithm must be WG_SORT_AUTO, WG_SORT_LSD or WG_SORT_BUCKET");
+    g_sort_algorithm.store(algo, std::memory_order_relaxed);
+  });
+}
+
+int wg_last_sort_algorithm(void) { return t_last_sort; }
+
+}  // extern "C"

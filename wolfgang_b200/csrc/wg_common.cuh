@@ -177,6 +177,20 @@ void pool_free(void* p, cudaStream_t s) noexcept;
 // most significant) carrying a 32-bit item index (wg_simplify.cu).
 void radix_sort_keys(int device, size_t n, int K, Scratch& keys, Scratch& idx, cudaStream_t s);
 
+// Bucketed sort-reduce (wg_bucket.cu).  thr_mode: 0 cull at thr_fixed, 1 at
+// atol + rtol*max|c|, 2 at atol (empty result when some |c| is infinite).
+// Each returns false when the inputs are outside the bucketed path's limits;
+// the caller then runs the LSD pipeline.
+bool bucket_products(int device, int W, const uint64_t* lx, const uint64_t* lz, const double* lc, size_t n_l,
+                     const uint64_t* rx, const uint64_t* rz, const double* rc, size_t n_r, int thr_mode, double atol,
+                     double rtol, double thr_fixed, uint64_t** ox, uint64_t** oz, double** oc, size_t* U,
+                     cudaStream_t s);
+bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, const double* c, size_t n,
+                     int thr_mode, double atol, double rtol, uint64_t** ox, uint64_t** oz, double** oc, size_t* U,
+                     cudaStream_t s);
+int sort_algorithm();     // WG_SORT_* setting
+void note_sort(int algo);  // records the algorithm of the thread's last result
+
 inline size_t checked_mul(size_t a, size_t b, const char* what) {
   if (a != 0 && b > SIZE_MAX / a) throw_invalid(std::string(what) + " size overflows size_t");
   return a * b;

@@ -411,6 +411,14 @@ double threshold(double atol, double rtol, unsigned long long max_bits) {
   return atol + prod;
 }
 
+// Bucketed sort-reduce for 1-2 mask words: chosen by WG_SORT_BUCKET, or by
+// WG_SORT_AUTO from 2^20 items on (below that the LSD passes are cheap).
+bool use_bucket(int W, size_t n) {
+  const int algo = wg::sort_algorithm();
+  if (algo == WG_SORT_LSD || W < 1 || W > 2) return false;
+  return algo == WG_SORT_BUCKET || n >= (size_t{1} << 20);
+}
+
 void validate_tolerances(double atol, double rtol) {
   // src/simplify.cpp:148-150
   if (atol < 0.0 || rtol < 0.0 || !std::isfinite(atol) || !std::isfinite(rtol))
@@ -459,6 +467,13 @@ int wg_simplify(int device, size_t words, size_t n_terms, const uint64_t* x, con
     wg::DeviceGuard g(device);
     cudaStream_t s = stream;
     const int W = static_cast<int>(words);
+    if (use_bucket(W, n_terms) &&
+        wg::bucket_simplify(device, W, x, z, coeffs, n_terms, rtol > 0.0 ? 1 : 2, atol, rtol, out_x, out_z,
+                            out_coeffs, out_terms, s)) {
+      wg::note_sort(WG_SORT_BUCKET);
+      return;
+    }
+    wg::note_sort(WG_SORT_LSD);
     wg::Scratch mx(sizeof(unsigned long long), s);
     wg::check_cuda(cudaMemsetAsync(mx.get(), 0, sizeof(unsigned long long), s), "clear max");
     WG_TIMED("max_abs_kernel", s,
@@ -506,6 +521,16 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x, const uin
       *out_terms = P;
       return;
     }
+    // The fused hash path of the reference culls at a hard-coded 1e-12
+    // (src/multiply.cpp:144, :226); simplify() uses atol + rtol*max|c|.
+    const int thr_mode = mode == WG_PRODUCTS_FUSED ? 0 : (rtol > 0.0 ? 1 : 2);
+    if (use_bucket(W, P) &&
+        wg::bucket_products(device, W, lhs_x, lhs_z, lhs_c, n_lhs, rhs_x, rhs_z, rhs_c, n_rhs, thr_mode, atol, rtol,
+                            1.0e-12, out_x, out_z, out_coeffs, out_terms, s)) {
+      wg::note_sort(WG_SORT_BUCKET);
+      return;
+    }
+    wg::note_sort(WG_SORT_LSD);
     wg::Scratch keys(sizeof(uint64_t) * std::max<size_t>(1, 2 * words * P), s);
     wg::Scratch idx(sizeof(uint32_t) * P, s);
     wg::Scratch pc(sizeof(double) * 2 * P, s);
@@ -515,8 +540,6 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x, const uin
     products_dispatch(W, lhs_x, lhs_z, lhs_c, n_lhs, rhs_x, rhs_z, rhs_c, n_rhs, keys.as<uint64_t>(),
                       idx.as<uint32_t>(), nullptr, nullptr, pc.as<double>(),
                       need_max ? mx.as<unsigned long long>() : nullptr, device, s);
-    // The fused hash path of the reference culls at a hard-coded 1e-12
-    // (src/multiply.cpp:144, :226); simplify() uses atol + rtol*max|c|.
     const double thr = need_max ? threshold(atol, rtol, read_scalar(mx.as<unsigned long long>(), s)) : 1.0e-12;
     sort_reduce(device, W, P, keys, idx, pc.as<double>(), thr, Outputs{out_x, out_z, out_coeffs, out_terms}, s);
   });
