@@ -5,7 +5,7 @@ The public operator types mirror the reference's ``wolfgang_quantum`` module:
 helpers.  Compute methods run on the GPU through the wg_* C-ABI of
 ``lib/libwgpauli.so``; there is no CPU fallback, and importing this package
 fails loudly when the native module has not been built
-(``python -m wolfgang_b200.build``).
+(``python wolfgang_b200/build.py``).
 """
 
 from __future__ import annotations
@@ -18,7 +18,7 @@ try:
     from . import _wolfgang_core  # noqa: F401
 except ImportError as exc:  # pragma: no cover - exercised only on a broken install
     raise ImportError(
-        "wolfgang_b200 native module is not built; run `python -m wolfgang_b200.build` "
+        "wolfgang_b200 native module is not built; run `python wolfgang_b200/build.py` "
         f"(sm_100a CUDA toolchain required): {exc}"
     ) from exc
 

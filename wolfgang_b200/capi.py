@@ -102,7 +102,7 @@ def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
         if not LIB_PATH.exists():
-            raise ImportError(f"{LIB_PATH} is not built; run `python -m wolfgang_b200.build`")
+            raise ImportError(f"{LIB_PATH} is not built; run `python wolfgang_b200/build.py`")
         L = ctypes.CDLL(str(LIB_PATH))
         for name, args in _SIGNATURES.items():
             fn = getattr(L, name)
