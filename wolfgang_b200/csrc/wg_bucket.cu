@@ -45,12 +45,14 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
 #include "wg_common.cuh"
+#include "wg_scan.cuh"
 
 namespace {
 
@@ -77,16 +79,11 @@ constexpr int kDistinct = 16;                   // distinct keys in one tie of 1
 constexpr uint32_t kExactBit = 1u << 31;        // fine bucket codes are exact (equal code = equal key)
 constexpr uint32_t kPureBit = 1u << 30;         // every key of the fine bucket is equal
 constexpr uint32_t kCountMask = kPureBit - 1;
-constexpr unsigned kFlagTimeout = 2u;
 constexpr unsigned kFlagOverrun = 4u;           // an output rank beyond capacity (internal error)
 constexpr unsigned kFlagCoarseFull = 8u;        // fallbacks: a coarse region over capacity,
 constexpr unsigned kFlagFineFull = 16u;         //   a fine bucket over kCap items (not of one key),
 constexpr unsigned kFlagDistinct = 32u;         //   a tie of more than kDistinct keys
 constexpr unsigned kFallbackMask = kFlagCoarseFull | kFlagFineFull | kFlagDistinct;
-constexpr unsigned kSpinLimit = 1u << 22;       // look-back polls (~0.5 s with back-off)
-constexpr unsigned long long kStAgg = 1ull << 62;
-constexpr unsigned long long kStIncl = 2ull << 62;
-constexpr unsigned long long kStValue = (1ull << 62) - 1;
 
 struct Control {
   unsigned k2_ticket;
@@ -97,7 +94,9 @@ struct Control {
   double thr;
   unsigned long long survivors;
   unsigned fine_total;
-  unsigned max_fine;  // largest fine bucket
+  unsigned max_fine;             // largest fine bucket
+  unsigned long long tie_items;  // items in runs of equal 8-digit codes (traced runs)
+  unsigned long long phase[4];   // final-kernel cycles per phase (traced runs)
 };
 
 // ------------------------------------------------------------------ keys and codes
@@ -543,7 +542,8 @@ struct FineParams {
   const int* Lj;              // prefix | dense << 16
   const uint32_t* idx_in;     // [B1][capc]
   uint16_t* fid_tmp;          // [B1][capc] fine bucket of each item
-  uint64_t* rec_code;         // [B1][capc] in fine-bucket order
+  uint32_t rstride;           // record region per coarse bucket (multiple of 32)
+  uint64_t* rec_code;         // [B1][rstride] in fine-bucket order, buckets 32-aligned
   uint32_t* rec_idx;
   uint32_t* fine_start;       // [G]
   uint32_t* fine_count;       // [G] count | kExactBit | kPureBit
@@ -592,6 +592,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     if (j >= P.B1) break;
     const uint32_t n = min(P.fill[j], P.capc);
     const size_t base = static_cast<size_t>(j) * P.capc;
+    const size_t rbase = static_cast<size_t>(j) * P.rstride;
     const uint32_t g0 = P.fine_base[j];
     const int slots = static_cast<int>(P.fine_base[j + 1] - g0);
     const int target = static_cast<int>(fine_target(n));
@@ -665,18 +666,19 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       warp_aggregated_add(cnt, static_cast<unsigned>(f), valid);
     }
     __syncthreads();
-    // fine bucket offsets (slots <= 1024: one or two rounds of the block scan)
+    // fine bucket offsets, each bucket starting on a multiple of 32 records
+    // (slots <= 1024: one or two rounds of the block scan)
     unsigned carry = 0;
     for (int f0 = 0; f0 < slots; f0 += blockDim.x) {
       const int f = f0 + threadIdx.x;
       const unsigned c = f < slots ? cnt[f] : 0u;
       unsigned tot;
-      const unsigned ex = block_exclusive_scan(c, warp_tmp, &tot);
+      const unsigned ex = block_exclusive_scan((c + 31u) & ~31u, warp_tmp, &tot);
       if (f < slots) {
         const unsigned off = carry + ex;
         const bool exact = (fL[f] >> 16) & 1;
         const bool pure = exact && (fL[f] & 0xffff) == total;  // every key of the bucket is equal
-        P.fine_start[g0 + f] = static_cast<uint32_t>(base + off);
+        P.fine_start[g0 + f] = static_cast<uint32_t>(rbase + off);
         P.fine_count[g0 + f] = c | (exact ? kExactBit : 0u) | (pure ? kPureBit : 0u);
         P.fine_L[g0 + f] = static_cast<uint16_t>(fL[f] & 0xffff);
         cnt[f] = off;
@@ -695,8 +697,8 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
         uint64_t c[KW];
         src.ckey(p, c);
         const int Lf = fL[f];
-        P.rec_code[base + pos] = code_of<KW>(c, Lf & 0xffff, (Lf >> 16) & 1);
-        P.rec_idx[base + pos] = p;
+        P.rec_code[rbase + pos] = code_of<KW>(c, Lf & 0xffff, (Lf >> 16) & 1);
+        P.rec_idx[rbase + pos] = p;
       }
     }
     __syncthreads();
@@ -709,14 +711,14 @@ struct FinalParams {
   const uint32_t* fine_start;
   const uint32_t* fine_count;
   const uint16_t* fine_L;
-  const uint64_t* rec_code;
-  const uint32_t* rec_idx;
-  unsigned long long* state;  // look-back: flag | value per fine bucket
+  uint64_t* rec_code;
+  uint32_t* rec_idx;      // rewritten in sorted order
+  uint32_t* head_bits;    // [records / 32] segment heads (buckets are 32-aligned)
+  uint32_t* keep_bits;    // [records / 32] surviving segments
+  uint32_t* counts;       // [G] survivors per fine bucket
+  double* big_sum;        // [2G] sum of a fine bucket of one key above kCap items
   Control* ctl;
-  uint64_t* out_x;
-  uint64_t* out_z;
-  double* out_c;
-  size_t out_cap;  // terms the outputs hold
+  int trace;              // record per-phase cycles
 };
 
 struct FinalSmem {
@@ -724,13 +726,11 @@ struct FinalSmem {
   uint32_t idx[kPadded];
   uint32_t head[kWords];
   uint32_t keep[kWords];
-  uint32_t wpre[kWords];
   uint32_t runs[kMaxRuns];  // start << 16 | end of tie runs
   unsigned n_runs;
   unsigned warp_sum[kK3Threads / 32];
   unsigned job;
   unsigned kept;
-  unsigned long long excl;
 };
 
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
@@ -1054,7 +1054,9 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
   const unsigned G = P.ctl->fine_total;
   const double thr = P.ctl->thr;
   bool inf = false;
+  long long tp[5] = {0, 0, 0, 0, 0};
   while (true) {
+    if (P.trace && tid == 0) tp[0] = clock64();
     if (tid == 0) S.job = atomicAdd(&P.ctl->k3_ticket, 1u);
     __syncthreads();
     const unsigned g = S.job;
@@ -1066,31 +1068,31 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
     const bool exact = (cw & kExactBit) != 0;
     const bool pure = (cw & kPureBit) != 0;
     const bool fits = n <= kCap;
-    unsigned count = 0;
     if (tid == 0 && n > 0) {
       if (!fits && !pure) atomicOr(&P.ctl->flags, kFlagFineFull);
       atomicMax(&P.ctl->max_fine, static_cast<unsigned>(n));
     }
-    c128 big_sum{0.0, 0.0};
-    uint32_t big_first = 0;
     if (!fits && pure) {
       // one key, more items than shared memory holds: sort the indices in
       // global memory, then one thread sums them in index order
-      uint32_t* a = const_cast<uint32_t*>(P.rec_idx) + start;
-      uint32_t* tmp = reinterpret_cast<uint32_t*>(const_cast<uint64_t*>(P.rec_code) + start);
+      uint32_t* a = P.rec_idx + start;
+      uint32_t* tmp = reinterpret_cast<uint32_t*>(P.rec_code + start);
       const uint32_t* sorted = radix_sort_u32(S, a, tmp, n);
       if (tid == 0) {
+        c128 acc{0.0, 0.0};
         for (int m = 0; m < n; ++m) {
           uint64_t k[KW];
           const c128 c = src.key_coeff(sorted[m], k);
           if (!(fabs(c.re) <= 0x1p1022 && fabs(c.im) <= 0x1p1022) && isinf(wgd::hypot_ref(c.re, c.im))) inf = true;
-          big_sum = wgd::cadd(big_sum, c);
+          acc = wgd::cadd(acc, c);
         }
-        big_first = sorted[0];
-        S.kept = wgd::hypot_ref(big_sum.re, big_sum.im) > thr ? 1u : 0u;
+        const bool kp = wgd::hypot_ref(acc.re, acc.im) > thr;
+        P.rec_idx[start] = sorted[0];
+        P.big_sum[2 * g] = acc.re;
+        P.big_sum[2 * g + 1] = acc.im;
+        P.counts[g] = kp ? 1u : 0u;
       }
       __syncthreads();
-      count = S.kept;
     }
     if (fits && n > 0) {
       int n_pad = kIPT;
@@ -1105,7 +1107,9 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
       }
       if (tid == 0) S.n_runs = 0;
       __syncthreads();
+      if (P.trace && tid == 0) tp[1] = clock64();
       block_merge_sort(S, n_pad);
+      if (P.trace && tid == 0) tp[2] = clock64();
       // segment heads where the code changes
       for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
         const int i = i0 + lane;
@@ -1124,6 +1128,7 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
           while (e < n && S.code[pidx(e)] == ci) ++e;
           const unsigned q = atomicAdd(&S.n_runs, 1u);
           S.runs[q] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(e);
+          if (P.trace) atomicAdd(&P.ctl->tie_items, static_cast<unsigned long long>(e - i));
         }
         __syncthreads();
         const int L = P.fine_L[g];
@@ -1133,20 +1138,32 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
                           &P.ctl->flags);
       }
       __syncthreads();
+      if (P.trace && tid == 0) tp[3] = clock64();
       // segment sums and the cull
       for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
         const int i = i0 + lane;
         bool kp = false;
         if (i < n && bit_at(S.head, i)) {
           const c128 s = segment_sum<KW>(src, S, i, next_set(S.head, i, n), inf);
-          kp = wgd::hypot_ref(s.re, s.im) > thr;
+          // without NaNs the rounded |s| is never below max(|re|, |im|), which
+          // decides most sums without the full hypot
+          const bool plain = !isnan(s.re) && !isnan(s.im);
+          kp = (plain && (fabs(s.re) > thr || fabs(s.im) > thr)) || wgd::hypot_ref(s.re, s.im) > thr;
         }
         const uint32_t b = __ballot_sync(0xffffffffu, kp);
         if (lane == 0) S.keep[i0 >> 5] = b;
       }
       __syncthreads();
+      // sorted indices, segment heads and survivors go back to global memory
+      // for the output pass
+      const int nw = (n + 31) >> 5;
+      for (int i = tid; i < n; i += kK3Threads) P.rec_idx[start + i] = S.idx[pidx(i)];
       unsigned c = 0;
-      for (int w = tid; w < (n + 31) / 32; w += kK3Threads) c += __popc(S.keep[w]);
+      for (int w = tid; w < nw; w += kK3Threads) {
+        P.head_bits[(start >> 5) + w] = S.head[w];
+        P.keep_bits[(start >> 5) + w] = S.keep[w];
+        c += __popc(S.keep[w]);
+      }
 #pragma unroll
       for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
       if (lane == 0) S.warp_sum[warp] = c;
@@ -1154,105 +1171,120 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
       if (tid == 0) {
         unsigned tsum = 0;
         for (int w = 0; w < kK3Threads / 32; ++w) tsum += S.warp_sum[w];
-        S.kept = tsum;
+        P.counts[g] = tsum;
       }
-      __syncthreads();
-      count = S.kept;
-    }
-    // decoupled look-back over the preceding fine buckets (bounded polling)
-    if (tid == 0) {
-      unsigned long long excl = 0;
-      if (g > 0) {
-        atomicExch(P.state + g, kStAgg | count);
-        long k = static_cast<long>(g) - 1;
-        unsigned polls = 0;
-        while (k >= 0) {
-          const unsigned long long v = *reinterpret_cast<volatile unsigned long long*>(P.state + k);
-          const unsigned long long fl = v & ~kStValue;
-          if (fl == 0) {
-            if (++polls > kSpinLimit) {
-              atomicOr(&P.ctl->flags, kFlagTimeout);
-              break;
-            }
-            __nanosleep(100);
-            continue;
-          }
-          excl += v & kStValue;
-          if (fl == kStIncl) break;
-          --k;
-        }
-      }
-      atomicExch(P.state + g, kStIncl | (excl + count));
-      if (g == G - 1) P.ctl->survivors = excl + count;
-      S.excl = excl;
-    }
-    __syncthreads();
-    if (!fits && pure && count > 0 && tid == 0) {
-      const size_t o = S.excl;
-      if (o >= P.out_cap) {
-        atomicOr(&P.ctl->flags, kFlagOverrun);
-      } else {
-        uint64_t k[KW];
-        src.key(big_first, k);
-#pragma unroll
-        for (int w = 0; w < KW / 2; ++w) {
-          P.out_x[o * (KW / 2) + w] = k[2 * w];
-          P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
-        }
-        P.out_c[2 * o] = big_sum.re;
-        P.out_c[2 * o + 1] = big_sum.im;
-      }
-    }
-    if (fits && count > 0) {
-      const int nw = (n + 31) / 32;
-      if (warp == 0) {
-        // exclusive prefix of survivors per bitmask word (at most 4 words per lane)
-        unsigned v[4], s = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int w = lane * 4 + q;
-          v[q] = w < nw ? __popc(S.keep[w]) : 0u;
-          s += v[q];
-        }
-        unsigned incl = s;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += y;
-        }
-        unsigned run = incl - s;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int w = lane * 4 + q;
-          if (w < nw) S.wpre[w] = run;
-          run += v[q];
-        }
-      }
-      __syncthreads();
-      const unsigned long long excl = S.excl;
-      for (int i = tid; i < n; i += kK3Threads) {
-        if (!bit_at(S.keep, i)) continue;
-        const size_t o = excl + S.wpre[i >> 5] + __popc(S.keep[i >> 5] & ((1u << (i & 31)) - 1u));
-        if (o >= P.out_cap) {
-          atomicOr(&P.ctl->flags, kFlagOverrun);
-          continue;
-        }
-        uint64_t k[KW];
-        src.key(S.idx[pidx(i)], k);
-        bool unused = false;
-        const c128 s = segment_sum<KW>(src, S, i, next_set(S.head, i, n), unused);
-#pragma unroll
-        for (int w = 0; w < KW / 2; ++w) {
-          P.out_x[o * (KW / 2) + w] = k[2 * w];
-          P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
-        }
-        P.out_c[2 * o] = s.re;
-        P.out_c[2 * o + 1] = s.im;
+      if (P.trace && tid == 0) {
+        tp[4] = clock64();
+        for (int q = 0; q < 4; ++q) atomicAdd(&P.ctl->phase[q], static_cast<unsigned long long>(tp[q + 1] - tp[q]));
       }
     }
     __syncthreads();
   }
   if (inf) atomicOr(&P.ctl->inf_seen, 1u);
+}
+
+// ------------------------------------------------------------------ output
+
+struct OutputParams {
+  const uint32_t* fine_start;
+  const uint32_t* fine_count;
+  const uint32_t* rec_idx;     // sorted within each fine bucket
+  const uint32_t* head_bits;
+  const uint32_t* keep_bits;
+  const uint32_t* offsets;     // [G] exclusive prefix of the survivor counts
+  const uint32_t* counts;
+  const double* big_sum;
+  const Control* ctl;
+  uint64_t* out_x;
+  uint64_t* out_z;
+  double* out_c;
+  size_t out_cap;
+  unsigned* flags;
+};
+
+// One CTA per fine bucket: each surviving segment head finds its output rank
+// from the bucket offset and the keep bits before it, sums its segment again
+// (the same additions in the same order) and writes key and coefficient.
+template <int KW, class Src>
+__global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParams P) {
+  __shared__ uint32_t hw[kWords], kw[kWords], wpre[kWords];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const unsigned G = P.ctl->fine_total;
+  for (unsigned g = blockIdx.x; g < G; g += gridDim.x) {
+    if (P.counts[g] == 0) continue;
+    const uint32_t start = P.fine_start[g];
+    const int n = static_cast<int>(P.fine_count[g] & kCountMask);
+    const size_t base_rank = P.offsets[g];
+    if (n > kCap) {
+      // a bucket of one key above kCap items: its sum was formed in order
+      if (tid == 0) {
+        if (base_rank >= P.out_cap) {
+          atomicOr(P.flags, kFlagOverrun);
+        } else {
+          uint64_t k[KW];
+          src.key(P.rec_idx[start], k);
+#pragma unroll
+          for (int w = 0; w < KW / 2; ++w) {
+            P.out_x[base_rank * (KW / 2) + w] = k[2 * w];
+            P.out_z[base_rank * (KW / 2) + w] = k[2 * w + 1];
+          }
+          P.out_c[2 * base_rank] = P.big_sum[2 * g];
+          P.out_c[2 * base_rank + 1] = P.big_sum[2 * g + 1];
+        }
+      }
+      continue;
+    }
+    const int nw = (n + 31) >> 5;
+    for (int w = tid; w < nw; w += blockDim.x) {
+      hw[w] = P.head_bits[(start >> 5) + w];
+      kw[w] = P.keep_bits[(start >> 5) + w];
+    }
+    __syncthreads();
+    if (tid < 32) {
+      // exclusive prefix of survivors per bitmask word (at most 4 words per lane)
+      unsigned v[4], s = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int w = lane * 4 + q;
+        v[q] = w < nw ? __popc(kw[w]) : 0u;
+        s += v[q];
+      }
+      unsigned incl = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      unsigned run = incl - s;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int w = lane * 4 + q;
+        if (w < nw) wpre[w] = run;
+        run += v[q];
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+      if (!bit_at(kw, i)) continue;
+      const size_t o = base_rank + wpre[i >> 5] + __popc(kw[i >> 5] & ((1u << (i & 31)) - 1u));
+      if (o >= P.out_cap) {
+        atomicOr(P.flags, kFlagOverrun);
+        continue;
+      }
+      const int e = next_set(hw, i, n);
+      uint64_t k[KW];
+      c128 acc{0.0, 0.0};
+      for (int m = i; m < e; ++m) acc = wgd::cadd(acc, src.key_coeff(P.rec_idx[start + m], k));  // one key
+#pragma unroll
+      for (int w = 0; w < KW / 2; ++w) {
+        P.out_x[o * (KW / 2) + w] = k[2 * w];
+        P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
+      }
+      P.out_c[2 * o] = acc.re;
+      P.out_c[2 * o + 1] = acc.im;
+    }
+    __syncthreads();
+  }
 }
 
 // ------------------------------------------------------------------ host side
@@ -1272,6 +1304,27 @@ struct Outs {
   size_t* n;
 };
 
+// Host-side stage times of one traced call (WG_BUCKET_TRACE set).
+struct Stamps {
+  bool on = std::getenv("WG_BUCKET_TRACE") != nullptr;
+  int k = 0;
+  const char* name[16];
+  std::chrono::steady_clock::time_point t[16];
+  void operator()(const char* what) {
+    if (on && k < 16) {
+      name[k] = what;
+      t[k++] = std::chrono::steady_clock::now();
+    }
+  }
+  ~Stamps() {
+    if (!on || k < 2) return;
+    std::fprintf(stderr, "bucket host stages (ms):");
+    for (int i = 1; i < k; ++i)
+      std::fprintf(stderr, " %s %.2f", name[i], std::chrono::duration<double, std::milli>(t[i] - t[i - 1]).count());
+    std::fprintf(stderr, "\n");
+  }
+};
+
 template <class K>
 void set_smem(K kernel, size_t bytes) {
   wg::check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
@@ -1281,6 +1334,8 @@ void set_smem(K kernel, size_t bytes) {
 template <int KW, class Src>
 bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec& thr, const Outs& out,
                 cudaStream_t s) {
+  Stamps stamp;
+  stamp("start");
   const int W = KW / 2;
   const bool dense0 = total <= 64;
   int B1 = 2;
@@ -1292,15 +1347,29 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   const size_t region = static_cast<size_t>(B1) * capc;
   // fine slots: sum over coarse buckets of t + t/4 + 8 with t <= n_j/kFineAvg + 1
   const size_t Gmax = (static_cast<size_t>(n) / kFineAvg + B1) * 5 / 4 + static_cast<size_t>(B1) * 9 + 1;
+  // records of the fine partition: rstride slots per coarse bucket, every fine
+  // bucket starting on a multiple of 32
+  const uint64_t rstride64 = ((static_cast<uint64_t>(capc) + 31) & ~uint64_t{31}) + 32ull * kFineSlots;
+  if (static_cast<uint64_t>(B1) * rstride64 >= 0xffffffffull) return false;
+  const uint32_t rstride = static_cast<uint32_t>(rstride64);
+  const size_t records = static_cast<size_t>(B1) * rstride;
   const auto& props = wg::device_props(device);
+  const bool trace = stamp.on;
 
-  wg::Scratch ctl(sizeof(Control), s);
-  wg::check_cuda(cudaMemsetAsync(ctl.get(), 0, sizeof(Control), s), "clear bucket control");
-  Control* dctl = ctl.as<Control>();
+  // every intermediate lives in the device workspace
+  using WS = wg::Workspace;
+  const size_t ws_bytes = WS::rounded(sizeof(Control)) + WS::rounded(8 * B1) + WS::rounded(4 * B1) +
+                          WS::rounded(4 * region) + WS::rounded(4 * (B1 + 1)) + WS::rounded(4 * B1) +
+                          WS::rounded(8 * records) + WS::rounded(4 * records) + 2 * WS::rounded(4 * Gmax) +
+                          WS::rounded(2 * Gmax) + WS::rounded(2 * region) + 2 * WS::rounded(records / 8) +
+                          2 * WS::rounded(4 * Gmax) + WS::rounded(16 * Gmax) + WS::rounded(4);
+  WS ws(device, ws_bytes, s);
+  Control* dctl = ws.take_as<Control>(1);
+  wg::check_cuda(cudaMemsetAsync(dctl, 0, sizeof(Control), s), "clear bucket control");
 
   // coarse splitters from a sorted sample of codes
   const uint32_t S1 = static_cast<uint32_t>(std::min<uint64_t>(n, static_cast<uint64_t>(kCoarseSample) * B1));
-  wg::Scratch split(sizeof(uint64_t) * B1, s);
+  uint64_t* split = ws.take_as<uint64_t>(B1);
   {
     wg::Scratch skeys(sizeof(uint64_t) * S1, s), sidx(sizeof(uint32_t) * S1, s);
     WG_TIMED("bucket_sample_kernel", s,
@@ -1310,36 +1379,39 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
     wg::check_launch("launch bucket sample");
     wg::radix_sort_keys(device, S1, 1, skeys, sidx, s);
     WG_TIMED("bucket_pick_kernel", s,
-      bucket_pick_kernel<<<(B1 + 255) / 256, 256, 0, s>>>(skeys.as<uint64_t>(), S1, B1, split.as<uint64_t>()));
+      bucket_pick_kernel<<<(B1 + 255) / 256, 256, 0, s>>>(skeys.as<uint64_t>(), S1, B1, split));
     wg::check_launch("launch bucket splitters");
   }
+  stamp("sample");
 
   // coarse scatter
-  wg::Scratch fill(sizeof(unsigned) * B1, s), idx1(sizeof(uint32_t) * region, s);
-  wg::check_cuda(cudaMemsetAsync(fill.get(), 0, sizeof(unsigned) * B1, s), "clear coarse fill");
+  unsigned* fill = ws.take_as<unsigned>(B1);
+  uint32_t* idx1 = ws.take_as<uint32_t>(region);
+  wg::check_cuda(cudaMemsetAsync(fill, 0, sizeof(unsigned) * B1, s), "clear coarse fill");
   {
-    const CoarseParams cp{split.as<uint64_t>(), B1, capc, fill.as<unsigned>(), idx1.as<uint32_t>(), dense0,
-                          thr.mode == 1, &dctl->max_bits};
+    const CoarseParams cp{split, B1, capc, fill, idx1, dense0, thr.mode == 1, &dctl->max_bits};
     const unsigned grid = wg::grid_for(n, kK1Threads * kK1Items, device, 2);
     WG_TIMED("bucket_coarse_kernel", s, bucket_coarse_kernel<KW><<<grid, kK1Threads, 0, s>>>(src, n, cp));
     wg::check_launch("launch coarse scatter");
   }
-  wg::Scratch fine_base(sizeof(uint32_t) * (B1 + 1), s), Lj(sizeof(int) * B1, s);
+  uint32_t* fine_base = ws.take_as<uint32_t>(B1 + 1);
+  int* Lj = ws.take_as<int>(B1);
   WG_TIMED("bucket_plan_kernel", s,
-    bucket_plan_kernel<<<1, 1024, 0, s>>>(fill.as<unsigned>(), B1, capc, split.as<uint64_t>(), total, dense0,
-                                          thr.mode, thr.atol, thr.rtol, thr.fixed, dctl, fine_base.as<uint32_t>(),
-                                          Lj.as<int>()));
+    bucket_plan_kernel<<<1, 1024, 0, s>>>(fill, B1, capc, split, total, dense0, thr.mode, thr.atol, thr.rtol,
+                                          thr.fixed, dctl, fine_base, Lj));
   wg::check_launch("launch bucket plan");
+  stamp("coarse");
 
   // fine partition
-  wg::Scratch rec_code(sizeof(uint64_t) * region, s), rec_idx(sizeof(uint32_t) * region, s);
-  wg::Scratch fine_start(sizeof(uint32_t) * Gmax, s), fine_count(sizeof(uint32_t) * Gmax, s),
-      fine_L(sizeof(uint16_t) * Gmax, s);
+  uint64_t* rec_code = ws.take_as<uint64_t>(records);
+  uint32_t* rec_idx = ws.take_as<uint32_t>(records);
+  uint32_t* fine_start = ws.take_as<uint32_t>(Gmax);
+  uint32_t* fine_count = ws.take_as<uint32_t>(Gmax);
+  uint16_t* fine_L = ws.take_as<uint16_t>(Gmax);
   {
-    wg::Scratch fid_tmp(sizeof(uint16_t) * region, s);
-    const FineParams fp{fill.as<unsigned>(), capc, B1, total, fine_base.as<uint32_t>(), Lj.as<int>(),
-                        idx1.as<uint32_t>(), fid_tmp.as<uint16_t>(), rec_code.as<uint64_t>(), rec_idx.as<uint32_t>(),
-                        fine_start.as<uint32_t>(), fine_count.as<uint32_t>(), fine_L.as<uint16_t>(), dctl};
+    uint16_t* fid_tmp = ws.take_as<uint16_t>(region);
+    const FineParams fp{fill, capc, B1, total, fine_base, Lj, idx1, fid_tmp, rstride, rec_code, rec_idx,
+                        fine_start, fine_count, fine_L, dctl};
     auto* k2 = bucket_fine_kernel<KW, Src>;
     set_smem(k2, kK2Smem);
     int per_sm = 0;
@@ -1349,17 +1421,19 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
     WG_TIMED("bucket_fine_kernel", s, k2<<<grid, kK2Threads, kK2Smem, s>>>(src, fp));
     wg::check_launch("launch fine partition");
   }
-  idx1.release();
+  stamp("fine");
 
-  // final: outputs at capacity n (shrunk below when far fewer survive)
-  const size_t nn = n;
-  wg::Scratch ox(sizeof(uint64_t) * W * nn, s), oz(sizeof(uint64_t) * W * nn, s), oc(sizeof(double) * 2 * nn, s);
-  wg::Scratch state(sizeof(unsigned long long) * Gmax, s);
-  wg::check_cuda(cudaMemsetAsync(state.get(), 0, sizeof(unsigned long long) * Gmax, s), "clear look-back state");
+  // final: sort, reduce and cull each fine bucket; survivors per bucket
+  uint32_t* head_bits = ws.take_as<uint32_t>(records / 32);
+  uint32_t* keep_bits = ws.take_as<uint32_t>(records / 32);
+  uint32_t* counts = ws.take_as<uint32_t>(Gmax);
+  uint32_t* offsets = ws.take_as<uint32_t>(Gmax);
+  double* big_sum = ws.take_as<double>(2 * Gmax);
+  uint32_t* survivors = ws.take_as<uint32_t>(1);
+  wg::check_cuda(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * Gmax, s), "clear survivor counts");
   {
-    const FinalParams fp{fine_start.as<uint32_t>(), fine_count.as<uint32_t>(), fine_L.as<uint16_t>(),
-                         rec_code.as<uint64_t>(), rec_idx.as<uint32_t>(), state.as<unsigned long long>(), dctl,
-                         ox.as<uint64_t>(), oz.as<uint64_t>(), oc.as<double>(), nn};
+    const FinalParams fp{fine_start, fine_count, fine_L, rec_code, rec_idx, head_bits, keep_bits, counts, big_sum,
+                         dctl, trace ? 1 : 0};
     auto* k3 = bucket_final_kernel<KW, Src>;
     set_smem(k3, sizeof(FinalSmem));
     int per_sm = 0;
@@ -1369,35 +1443,43 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
     WG_TIMED("bucket_final_kernel", s, k3<<<grid, kK3Threads, sizeof(FinalSmem), s>>>(src, fp));
     wg::check_launch("launch bucket final");
   }
+  wgs::exclusive_scan<uint32_t>(counts, offsets, Gmax, survivors, s);
+  stamp("final");
   Control h{};
+  uint32_t U32 = 0;
   wg::check_cuda(cudaMemcpyAsync(&h, dctl, sizeof(Control), cudaMemcpyDeviceToHost, s), "read bucket control");
+  wg::check_cuda(cudaMemcpyAsync(&U32, survivors, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+                 "read survivor count");
   wg::check_cuda(cudaStreamSynchronize(s), "synchronize bucket sort");
-  if (std::getenv("WG_BUCKET_TRACE"))
-    std::fprintf(stderr, "bucket: n=%u coarse=%d fine=%u max_fine=%u flags=0x%x survivors=%llu\n", n, B1,
-                 h.fine_total, h.max_fine, h.flags, h.survivors);
-  if (h.flags & kFlagTimeout)
-    throw wg::Error(WG_ERR_TIMEOUT, "bucketed simplify: a fine bucket waited too long for its predecessors");
-  if (h.flags & kFlagOverrun) throw wg::Error(WG_ERR_CUDA, "bucketed simplify: output rank beyond capacity");
+  stamp("sync");
+  if (trace) {
+    std::fprintf(stderr, "bucket: n=%u coarse=%d fine=%u max_fine=%u flags=0x%x survivors=%u tie_items=%llu\n", n, B1,
+                 h.fine_total, h.max_fine, h.flags, U32, h.tie_items);
+    std::fprintf(stderr, "bucket final phases (Gcycles, all CTAs): load %.2f sort %.2f ties %.2f sums %.2f\n",
+                 h.phase[0] * 1e-9, h.phase[1] * 1e-9, h.phase[2] * 1e-9, h.phase[3] * 1e-9);
+  }
   if (h.flags & kFallbackMask) return false;
-  size_t U = static_cast<size_t>(h.survivors);
+  size_t U = U32;
   if (thr.mode == 2 && h.inf_seen) U = 0;  // atol + 0 * inf is NaN: nothing survives
   *out.n = U;
   *out.x = *out.z = nullptr;
   *out.c = nullptr;
   if (U == 0) return true;
-  if (U < nn / 4 * 3) {
-    wg::Scratch sx(sizeof(uint64_t) * W * U, s), sz(sizeof(uint64_t) * W * U, s), sc(sizeof(double) * 2 * U, s);
-    wg::check_cuda(cudaMemcpyAsync(sx.get(), ox.get(), sizeof(uint64_t) * W * U, cudaMemcpyDeviceToDevice, s),
-                   "shrink outputs");
-    wg::check_cuda(cudaMemcpyAsync(sz.get(), oz.get(), sizeof(uint64_t) * W * U, cudaMemcpyDeviceToDevice, s),
-                   "shrink outputs");
-    wg::check_cuda(cudaMemcpyAsync(sc.get(), oc.get(), sizeof(double) * 2 * U, cudaMemcpyDeviceToDevice, s),
-                   "shrink outputs");
-    std::swap(ox, sx);
-    std::swap(oz, sz);
-    std::swap(oc, sc);
+  // output: each survivor at its rank
+  wg::Scratch ox(sizeof(uint64_t) * W * U, s), oz(sizeof(uint64_t) * W * U, s), oc(sizeof(double) * 2 * U, s);
+  stamp("alloc");
+  {
+    const OutputParams op{fine_start, fine_count, rec_idx, head_bits, keep_bits, offsets, counts, big_sum, dctl,
+                          ox.as<uint64_t>(), oz.as<uint64_t>(), oc.as<double>(), U, &dctl->flags};
+    const unsigned grid = static_cast<unsigned>(props.sm_count * 8);
+    WG_TIMED("bucket_output_kernel", s, bucket_output_kernel<KW><<<grid, 256, 0, s>>>(src, op));
+    wg::check_launch("launch bucket output");
   }
+  unsigned flags = 0;
+  wg::check_cuda(cudaMemcpyAsync(&flags, &dctl->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "read flags");
   wg::check_cuda(cudaStreamSynchronize(s), "synchronize bucket outputs");
+  stamp("output");
+  if (flags & kFlagOverrun) throw wg::Error(WG_ERR_CUDA, "bucketed simplify: output rank beyond the survivor count");
   *out.x = static_cast<uint64_t*>(ox.detach());
   *out.z = static_cast<uint64_t*>(oz.detach());
   *out.c = static_cast<double*>(oc.detach());

@@ -173,6 +173,28 @@ struct DeviceGuard {
 void* pool_alloc(size_t bytes, cudaStream_t s);
 void pool_free(void* p, cudaStream_t s) noexcept;
 
+// Per-device grow-only workspace for an entry point's intermediates.  It is
+// held for the whole call (calls on one device take turns on it) and kept for
+// later calls, so large scratch of varying sizes does not fragment the memory
+// pool: every call that uses it synchronises its stream before returning.
+class Workspace {
+ public:
+  Workspace(int device, size_t bytes, cudaStream_t s);
+  ~Workspace();
+  Workspace(const Workspace&) = delete;
+  Workspace& operator=(const Workspace&) = delete;
+  // 256-byte aligned piece of the reserved bytes.
+  void* take(size_t bytes);
+  template <typename T>
+  T* take_as(size_t count) { return static_cast<T*>(take(sizeof(T) * count)); }
+  static size_t rounded(size_t bytes) { return (bytes + 255) & ~size_t{255}; }
+
+ private:
+  int device_;
+  char* p_ = nullptr;
+  char* end_ = nullptr;
+};
+
 // Stable LSD radix sort of n items by K structure-of-arrays key words (word 0
 // most significant) carrying a 32-bit item index (wg_simplify.cu).
 void radix_sort_keys(int device, size_t n, int K, Scratch& keys, Scratch& idx, cudaStream_t s);

@@ -134,6 +134,48 @@ void pool_free(void* p, cudaStream_t s) noexcept {
   }
 }
 
+namespace {
+constexpr int kMaxDevices = 64;
+struct WorkspaceSlot {
+  std::mutex mu;
+  void* base = nullptr;
+  size_t cap = 0;
+};
+WorkspaceSlot g_workspace[kMaxDevices];
+}  // namespace
+
+Workspace::Workspace(int device, size_t bytes, cudaStream_t s) : device_(device) {
+  if (device < 0 || device >= kMaxDevices) throw_invalid("CUDA device ordinal is out of range");
+  WorkspaceSlot& w = g_workspace[device];
+  w.mu.lock();
+  try {
+    if (w.cap < bytes) {
+      if (w.base) pool_free(w.base, s);
+      w.base = nullptr;
+      w.cap = 0;
+      // some headroom, so that slightly larger calls reuse the block
+      const size_t want = bytes + bytes / 8;
+      w.base = pool_alloc(want, s);
+      w.cap = want;
+    }
+  } catch (...) {
+    w.mu.unlock();
+    throw;
+  }
+  p_ = static_cast<char*>(w.base);
+  end_ = p_ + w.cap;
+}
+
+Workspace::~Workspace() { g_workspace[device_].mu.unlock(); }
+
+void* Workspace::take(size_t bytes) {
+  const size_t r = rounded(bytes);
+  if (static_cast<size_t>(end_ - p_) < r) throw Error(WG_ERR_INVALID, "internal: workspace piece exceeds its reservation");
+  void* out = p_;
+  p_ += r;
+  return out;
+}
+
 void Scratch::reset(size_t bytes, cudaStream_t s) {
   release();
   s_ = s;
