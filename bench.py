@@ -252,6 +252,12 @@ def bench_products(args, world, rank, torch) -> dict:
         "seg_head_kernel": P * (8 * 2 * W + 4),               # read keys, write flag
         "seg_reduce_kernel": P * (4 + 16) + U * 20,           # idx + gathered coefficient, sums
         "write_out_kernel": U * (8 * 2 * W + 16),
+        # bucketed path: an item is a 4-byte product index; codes are 8 bytes;
+        # operand gathers hit L2 and are not counted
+        "bucket_coarse_kernel": P * 4,                         # write the item index
+        "bucket_fine_kernel": P * (4 + 2 + 2 + 4 + 8 + 4),     # idx, fine id (w+r), idx, code + idx out
+        "bucket_final_kernel": P * (8 + 4 + 4) + P // 4,       # code + idx in, sorted idx out, bitmasks
+        "bucket_output_kernel": P * 4 + P // 4 + U * (8 * 2 * W + 16),  # idx, bitmasks, the U terms
     }
     peak, peak_kind = peaks()
     out = {

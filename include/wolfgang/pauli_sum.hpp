@@ -102,6 +102,13 @@ class PauliSum {
            std::vector<std::uint64_t> x, std::vector<std::uint64_t> z,
            std::vector<std::complex<double>> coeffs);
 
+  // Takes ownership of device result buffers (library-allocated) and copies
+  // them into a host PauliSum; their masks come from valid inputs, so they are
+  // not re-checked.
+  static PauliSum download_device_result(std::size_t num_qubits, std::size_t words, int device,
+                                         std::uint64_t* x, std::uint64_t* z, double* coeffs,
+                                         std::size_t num_terms);
+
   std::size_t num_qubits_;
   std::size_t words_;
   std::size_t num_terms_;

@@ -232,10 +232,8 @@ PauliSum PauliSum::scalar_multiply(std::complex<double> scalar) const {
 
 // ------------------------------------------------------------------ device compute
 
-namespace {
-
-PauliSum download_result(std::size_t n, std::size_t words, int device, std::uint64_t* ox, std::uint64_t* oz,
-                         double* oc, std::size_t U) {
+PauliSum PauliSum::download_device_result(std::size_t n, std::size_t words, int device, std::uint64_t* ox,
+                                          std::uint64_t* oz, double* oc, std::size_t U) {
   DeviceBuffer bx = DeviceBuffer::adopt(device, ox, U * words * 8);
   DeviceBuffer bz = DeviceBuffer::adopt(device, oz, U * words * 8);
   DeviceBuffer bc = DeviceBuffer::adopt(device, oc, U * 16);
@@ -245,10 +243,8 @@ PauliSum download_result(std::size_t n, std::size_t words, int device, std::uint
   bx.download(x.data(), x.size() * 8);
   bz.download(z.data(), z.size() * 8);
   bc.download(c.data(), c.size() * 16);
-  return PauliSum::from_packed(n, std::move(x), std::move(z), std::move(c));
+  return PauliSum(n, words, U, std::move(x), std::move(z), std::move(c));
 }
-
-}  // namespace
 
 PauliSum PauliSum::simplify(double atol, double rtol) const {
   if (atol < 0.0 || rtol < 0.0 || !std::isfinite(atol) || !std::isfinite(rtol))
@@ -261,7 +257,7 @@ PauliSum PauliSum::simplify(double atol, double rtol) const {
   std::size_t U = 0;
   abi::check(wg_simplify(dev, words_, num_terms_, d.x.as<std::uint64_t>(), d.z.as<std::uint64_t>(),
                          d.c.as<double>(), atol, rtol, &ox, &oz, &oc, &U, nullptr));
-  return download_result(num_qubits_, words_, dev, ox, oz, oc, U);
+  return download_device_result(num_qubits_, words_, dev, ox, oz, oc, U);
 }
 
 PauliSum PauliSum::matmul(const PauliSum& rhs, bool simplify_output, std::size_t max_intermediate_terms) const {
@@ -293,7 +289,7 @@ PauliSum PauliSum::matmul(const PauliSum& rhs, bool simplify_output, std::size_t
     bc.download(c.data(), c.size() * 16);
     return PauliSum(num_qubits_, words_, U, std::move(x), std::move(z), std::move(c));
   }
-  return download_result(num_qubits_, words_, dev, ox, oz, oc, U);
+  return download_device_result(num_qubits_, words_, dev, ox, oz, oc, U);
 }
 
 std::vector<std::uint8_t> PauliSum::commutes_with(const PauliSum& rhs,

@@ -173,6 +173,12 @@ struct DeviceGuard {
 void* pool_alloc(size_t bytes, cudaStream_t s);
 void pool_free(void* p, cudaStream_t s) noexcept;
 
+// Copies of at least kStagedMin bytes between the device and pageable host
+// memory run through pinned staging (wg_runtime.cu); both synchronise s.
+constexpr size_t kStagedMin = size_t{32} << 20;
+bool pinned_host(const void* p);
+void staged_copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
+
 // Per-device grow-only workspace for an entry point's intermediates.  It is
 // held for the whole call (calls on one device take turns on it) and kept for
 // later calls, so large scratch of varying sizes does not fragment the memory

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "wg_common.cuh"
@@ -134,6 +135,90 @@ void pool_free(void* p, cudaStream_t s) noexcept {
   }
 }
 
+// ------------------------------------------------------------ staged copies
+//
+// Large copies between the device and pageable host memory go through two
+// pinned 64 MiB staging buffers: the DMA engine fills (or drains) one while
+// host threads copy the other, so the transfer runs near the link rate
+// instead of the driver's single-threaded pageable path.
+namespace {
+constexpr size_t kStageBytes = size_t{64} << 20;
+struct Staging {
+  std::mutex mu;
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+};
+Staging g_staging;
+
+void parallel_memcpy(char* dst, const char* src, size_t bytes) {
+  static const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  if (nt == 1 || bytes < (size_t{4} << 20)) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t part = (bytes + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < nt; ++i) {
+    const size_t o = i * part;
+    if (o >= bytes) break;
+    const size_t len = std::min(part, bytes - o);
+    th.emplace_back([=] { std::memcpy(dst + o, src + o, len); });
+  }
+  std::memcpy(dst, src, std::min(part, bytes));
+  for (auto& t : th) t.join();
+}
+}  // namespace
+
+bool pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+void staged_copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_staging.mu);
+  for (int i = 0; i < 2; ++i) {
+    if (!g_staging.buf[i]) {
+      check_cuda(cudaHostAlloc(&g_staging.buf[i], kStageBytes, cudaHostAllocPortable), "allocate pinned staging");
+      check_cuda(cudaEventCreateWithFlags(&g_staging.done[i], cudaEventDisableTiming), "create staging event");
+    }
+  }
+  char* const d = static_cast<char*>(dst);
+  const char* const sp = static_cast<const char*>(src);
+  const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
+  auto len_of = [&](size_t k) { return std::min(kStageBytes, bytes - k * kStageBytes); };
+  if (kind == cudaMemcpyDeviceToHost) {
+    // DMA chunk k into buffer k%2 while the host drains chunk k-1
+    for (size_t k = 0; k <= chunks; ++k) {
+      if (k < chunks) {
+        char* b = static_cast<char*>(g_staging.buf[k & 1]);
+        check_cuda(cudaMemcpyAsync(b, sp + k * kStageBytes, len_of(k), cudaMemcpyDeviceToHost, s),
+                   "copy device buffer to staging");
+        check_cuda(cudaEventRecord(g_staging.done[k & 1], s), "record staging event");
+      }
+      if (k > 0) {
+        const size_t j = k - 1;
+        check_cuda(cudaEventSynchronize(g_staging.done[j & 1]), "wait for staging");
+        parallel_memcpy(d + j * kStageBytes, static_cast<const char*>(g_staging.buf[j & 1]), len_of(j));
+      }
+    }
+  } else {
+    // the host fills buffer k%2 once the DMA of chunk k-2 has drained it
+    for (size_t k = 0; k < chunks; ++k) {
+      if (k >= 2) check_cuda(cudaEventSynchronize(g_staging.done[k & 1]), "wait for staging");
+      char* b = static_cast<char*>(g_staging.buf[k & 1]);
+      parallel_memcpy(b, sp + k * kStageBytes, len_of(k));
+      check_cuda(cudaMemcpyAsync(d + k * kStageBytes, b, len_of(k), cudaMemcpyHostToDevice, s),
+                 "copy staging to device buffer");
+      check_cuda(cudaEventRecord(g_staging.done[k & 1], s), "record staging event");
+    }
+  }
+  check_cuda(cudaStreamSynchronize(s), "synchronize staged copy");
+}
+
 namespace {
 constexpr int kMaxDevices = 64;
 struct WorkspaceSlot {
@@ -255,6 +340,10 @@ int wg_memcpy_htod(int device, void* dst, const void* src, size_t bytes, wg_stre
   return guarded([&] {
     if (bytes == 0) return;
     DeviceGuard g(device);
+    if (bytes >= kStagedMin && !wg::pinned_host(src)) {
+      wg::staged_copy(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+      return;
+    }
     check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "copy host buffer to device");
   });
 }
@@ -263,6 +352,10 @@ int wg_memcpy_dtoh(int device, void* dst, const void* src, size_t bytes, wg_stre
   return guarded([&] {
     if (bytes == 0) return;
     DeviceGuard g(device);
+    if (bytes >= kStagedMin && !wg::pinned_host(dst)) {
+      wg::staged_copy(dst, src, bytes, cudaMemcpyDeviceToHost, stream);
+      return;
+    }
     check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream), "copy device buffer to host");
     check_cuda(cudaStreamSynchronize(stream), "synchronize copy to host");
   });
