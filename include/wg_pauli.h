@@ -89,7 +89,8 @@ int wg_profile_report(char* buf, size_t cap);
  * bits[row*pitch_words + c/32] bit (c%32) = 1 iff lhs term `row` commutes with
  * rhs term c; pitch_words >= ceil(n_rhs/32); padding bits are written 0.
  * algo: 0 = autotuned choice, 1 = popcount/LOP3 with warp-ballot packing,
- * 2 = bit-plane XOR over the lhs support.  All algos give identical bits. */
+ * 2 = bit-plane XOR over the lhs support (up to 256 qubits; above that the
+ * call uses 1).  All algos give identical bits. */
 int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x,
                         const uint64_t* lhs_z, size_t n_lhs, const uint64_t* rhs_x,
                         const uint64_t* rhs_z, size_t n_rhs, uint32_t* bits,

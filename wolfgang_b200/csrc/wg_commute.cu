@@ -131,7 +131,7 @@ __global__ void fill_ones_kernel(uint32_t* bits, size_t rows, size_t cols, size_
 // (lx_q ? Zplane_q[j] : 0) ^ (lz_q ? Xplane_q[j] : 0).  Per output word that
 // is ~weight(l) shared-memory reads instead of 32 * (4W LOP3 + POPC), so for
 // sparse terms the kernel is bound by the output write.
-constexpr int kPlaneWords = 32;  // output words per row per CTA (1024 columns)
+constexpr int kPlaneWords = 64;  // output words per row per CTA (2048 columns), two per lane
 
 template <int W>
 __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
@@ -166,32 +166,62 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
     }
   }
   __syncthreads();
-  uint32_t valid = 0xffffffffu;
-  {
-    const size_t c_first = col0 + 32 * static_cast<size_t>(lane);
-    if (c_first >= n_r) valid = 0;
-    else if (n_r - c_first < 32) valid = (1u << (n_r - c_first)) - 1u;
+  // lane covers output words 2*lane and 2*lane + 1 of the block
+  uint32_t valid[2];
+  bool write_ok[2];
+  size_t wi[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int j = 2 * lane + h;
+    const size_t c_first = col0 + 32 * static_cast<size_t>(j);
+    valid[h] = c_first >= n_r ? 0u : (n_r - c_first < 32 ? (1u << (n_r - c_first)) - 1u : 0xffffffffu);
+    wi[h] = static_cast<size_t>(blockIdx.x) * kPlaneWords + j;
+    write_ok[h] = wi[h] < words_needed;
   }
-  const size_t wi = static_cast<size_t>(blockIdx.x) * kPlaneWords + lane;
+  const uint2* pl2 = reinterpret_cast<const uint2*>(planes);
   const size_t row0 = static_cast<size_t>(blockIdx.y) * rows_per_cta;
   const size_t row1 = min(n_l, row0 + rows_per_cta);
-  for (size_t row = row0 + warp; row < row1; row += kWarps) {
-    uint32_t acc = 0;
+  // A warp takes 32 rows at a time: lane r loads row rbase + r (coalesced),
+  // then each row's masks are broadcast by shuffles.  Set X bits of the row
+  // select rhs Z planes and set Z bits select rhs X planes.
+  for (size_t rbase = row0 + 32 * static_cast<size_t>(warp); rbase < row1; rbase += 32 * kWarps) {
+    const size_t my = rbase + lane;
+    uint64_t mx[W], mz[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      const uint64_t ax = __ldg(lx + row * W + w);
-      const uint64_t az = __ldg(lz + row * W + w);
-      uint64_t sup = ax | az;
-      while (sup) {
-        const int b = __ffsll(static_cast<long long>(sup)) - 1;
-        sup &= sup - 1;
-        const int q = w * 64 + b;
-        const uint32_t mx = 0u - static_cast<uint32_t>((ax >> b) & 1u);  // lhs X on q -> rhs Z plane
-        const uint32_t mz = 0u - static_cast<uint32_t>((az >> b) & 1u);  // lhs Z on q -> rhs X plane
-        acc ^= (planes[(q * 2 + 1) * kPlaneWords + lane] & mx) ^ (planes[(q * 2 + 0) * kPlaneWords + lane] & mz);
+      mx[w] = my < row1 ? __ldg(lx + my * W + w) : 0;
+      mz[w] = my < row1 ? __ldg(lz + my * W + w) : 0;
+    }
+    const int nrows = row1 - rbase < 32 ? static_cast<int>(row1 - rbase) : 32;
+    for (int rr = 0; rr < nrows; ++rr) {
+      uint2 acc = make_uint2(0u, 0u);
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        const uint64_t ax = __shfl_sync(0xffffffffu, mx[w], rr);
+        const uint64_t az = __shfl_sync(0xffffffffu, mz[w], rr);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          const int qb = w * 64 + half * 32;
+          for (uint32_t m = static_cast<uint32_t>(ax >> (32 * half)); m; m &= m - 1) {
+            const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 1) * (kPlaneWords / 2) + lane];
+            acc.x ^= v.x;
+            acc.y ^= v.y;
+          }
+          for (uint32_t m = static_cast<uint32_t>(az >> (32 * half)); m; m &= m - 1) {
+            const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 0) * (kPlaneWords / 2) + lane];
+            acc.x ^= v.x;
+            acc.y ^= v.y;
+          }
+        }
+      }
+      const size_t rowoff = (rbase + rr) * pitch;
+      if (write_ok[0] && write_ok[1] && (reinterpret_cast<uintptr_t>(bits + rowoff + wi[0]) & 7) == 0) {
+        *reinterpret_cast<uint2*>(bits + rowoff + wi[0]) = make_uint2(~acc.x & valid[0], ~acc.y & valid[1]);
+      } else {
+        if (write_ok[0]) bits[rowoff + wi[0]] = ~acc.x & valid[0];
+        if (write_ok[1]) bits[rowoff + wi[1]] = ~acc.y & valid[1];
       }
     }
-    if (wi < words_needed) bits[row * pitch + wi] = ~acc & valid;
   }
 }
 
@@ -232,7 +262,7 @@ void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint
   // Enough row chunks to fill the machine; rows per CTA amortise plane building.
   const size_t sms = wg::device_props(device).sm_count;
   size_t rows_per_cta = 2048;
-  while (rows_per_cta > 64 && col_blocks * ((n_l + rows_per_cta - 1) / rows_per_cta) < 4 * sms)
+  while (rows_per_cta > 256 && col_blocks * ((n_l + rows_per_cta - 1) / rows_per_cta) < 4 * sms)
     rows_per_cta /= 2;
   size_t row_chunks = (n_l + rows_per_cta - 1) / rows_per_cta;
   while (row_chunks > 65535) {
