@@ -146,9 +146,12 @@ def test_bucket_tie_heavy_position_codes(cuda, oracle, algo):
     assert same(got, oracle.simplify(120, *raw, 1e-12, 0.0))
 
 
-@pytest.mark.parametrize("copies,bucketed", [(3500, True), (5000, False)])
+@pytest.mark.parametrize("copies,bucketed", [(1500, True), (3500, True), (5000, True)])
 def test_bucket_one_key_runs(cuda, oracle, algo, copies, bucketed):
-    """One key repeated: one fine bucket (at most 4096 items) or a fallback."""
+    """One key of 14 set bits repeated: its eight-digit code does not fix the
+    key, so the run's fine bucket is checked key by key; up to 2048 items it is
+    sorted in shared memory, above that its indices are sorted in global
+    memory and summed in order."""
     rng = seeded("bucket-run", copies)
     n = 40
     x = np.zeros((copies + 300, 1), np.uint64)

@@ -32,10 +32,14 @@
 //          bucket's L, index) in fine order;
 //  final   fine buckets in global order, at most kCap items each: shared-memory
 //          merge sort by (code, index), tie runs reordered by (next code,
-//          index) and if need be by (key, index), equal-key runs summed left to
-//          right and culled, survivors written at an offset from a decoupled
-//          look-back over the preceding buckets.  A bucket of one key of any
-//          size has its indices radix-sorted in global memory instead.
+//          index) and if need be by (key, index); every item's coefficient is
+//          formed, equal-key runs are summed left to right from shared memory
+//          and culled, and the survivors (index, sum) are compacted at the
+//          start of the bucket's record range with their count.  A bucket of
+//          one key above kCap items has its indices radix-sorted in global
+//          memory instead and is summed by one thread;
+//  output  after a scan of the counts, one warp per fine bucket copies its
+//          survivors to their ranks, each key rebuilt from its operands.
 //
 // Anything outside this path's limits (more than 255 significant bits, a
 // coarse region or fine bucket over capacity, a tie of more than 16 different
@@ -61,17 +65,18 @@ using wgd::c128;
 constexpr int kCoarseLog = 18;           // about 2^18 items per coarse bucket
 constexpr int kCoarseMax = 2048;         // coarse buckets
 constexpr int kCoarseSample = 128;       // samples per coarse bucket
-constexpr int kFineAvg = 1536;           // target items per fine bucket
-constexpr int kFineMax = 512;            // target fine buckets per coarse bucket
-constexpr int kFineSlots = 1024;         // fine bucket slots per coarse bucket (targets + isolated codes)
-constexpr int kSample2 = 4096;           // in-bucket sample for fine splitters
+constexpr int kFineAvg = 640;            // target items per fine bucket
+constexpr int kFineMax = 896;            // target fine buckets per coarse bucket
+constexpr int kFineSlots = 1152;         // fine bucket slots per coarse bucket (targets + isolated codes)
+constexpr int kSample2 = 8192;           // in-bucket sample for fine splitters (about 20 per fine bucket)
 constexpr int kHeavyRun = 3;             // sample repeats that may isolate a code
 constexpr int kK1Threads = 512;
 constexpr int kK1Items = 16;
 constexpr int kK2Threads = 512;
 constexpr int kK3Threads = 256;
-constexpr int kIPT = 16;                        // items per thread in the final sort
-constexpr int kCap = kK3Threads * kIPT;         // 4096 items per fine bucket
+constexpr int kK3PerSM = 4;                     // final-kernel CTAs resident per SM
+constexpr int kIPT = 8;                         // items per thread in the final sort
+constexpr int kCap = kK3Threads * kIPT;         // 2048 items per fine bucket
 constexpr int kPadded = kCap + kCap / 16;       // one spare slot per 16 (bank spread)
 constexpr int kWords = kCap / 32;
 constexpr int kMaxRuns = kCap / 2;              // tie runs per bucket (runs have >= 2 items)
@@ -667,7 +672,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     }
     __syncthreads();
     // fine bucket offsets, each bucket starting on a multiple of 32 records
-    // (slots <= 1024: one or two rounds of the block scan)
+    // (slots <= kFineSlots: a few rounds of the block scan)
     unsigned carry = 0;
     for (int f0 = 0; f0 < slots; f0 += blockDim.x) {
       const int f = f0 + threadIdx.x;
@@ -711,26 +716,25 @@ struct FinalParams {
   const uint32_t* fine_start;
   const uint32_t* fine_count;
   const uint16_t* fine_L;
-  uint64_t* rec_code;
-  uint32_t* rec_idx;      // rewritten in sorted order
-  uint32_t* head_bits;    // [records / 32] segment heads (buckets are 32-aligned)
-  uint32_t* keep_bits;    // [records / 32] surviving segments
+  uint64_t* rec_code;     // codes in; real parts of the survivors' sums out
+  uint32_t* rec_idx;      // indices in; survivors' indices out (bucket start + rank)
+  double* rec_im;         // imaginary parts of the survivors' sums
   uint32_t* counts;       // [G] survivors per fine bucket
-  double* big_sum;        // [2G] sum of a fine bucket of one key above kCap items
   Control* ctl;
   int trace;              // record per-phase cycles
 };
 
 struct FinalSmem {
-  uint64_t code[kPadded];
+  uint64_t code[kPadded];   // codes; once sorted and tied, the real parts of coefficients and sums
+  double im[kPadded];       // imaginary parts of coefficients and sums
   uint32_t idx[kPadded];
   uint32_t head[kWords];
   uint32_t keep[kWords];
+  uint32_t wpre[kWords];    // survivors before each keep word
   uint32_t runs[kMaxRuns];  // start << 16 | end of tie runs
   unsigned n_runs;
-  unsigned warp_sum[kK3Threads / 32];
   unsigned job;
-  unsigned kept;
+  long long tp[5];          // phase clocks of traced runs
 };
 
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
@@ -755,98 +759,98 @@ __device__ __forceinline__ int next_set(const uint32_t* m, int i, int n) {
   return min(n, (w << 5) + __ffs(v) - 1);
 }
 
-__device__ __forceinline__ void reg_sort16(uint64_t (&c)[kIPT], uint32_t (&x)[kIPT]) {
-#pragma unroll
-  for (int k = 2; k <= kIPT; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-#pragma unroll
-      for (int i = 0; i < kIPT; ++i) {
-        const int l = i ^ j;
-        if (l > i) {
-          const bool up = (i & k) == 0;
-          const bool sw = up ? rec_less(c[l], x[l], c[i], x[i]) : rec_less(c[i], x[i], c[l], x[l]);
-          const uint64_t ci = c[i], cl = c[l];
-          const uint32_t xi = x[i], xl = x[l];
-          c[i] = sw ? cl : ci;
-          c[l] = sw ? ci : cl;
-          x[i] = sw ? xl : xi;
-          x[l] = sw ? xi : xl;
-        }
-      }
-    }
-  }
+// Compare-exchange of a pair of records: (c0, x0) takes the smaller when up,
+// the larger otherwise.
+__device__ __forceinline__ void cas(uint64_t& c0, uint32_t& x0, uint64_t& c1, uint32_t& x1, bool up) {
+  const bool sw = up == rec_less(c1, x1, c0, x0);
+  const uint64_t tc = c0;
+  const uint32_t tx = x0;
+  c0 = sw ? c1 : c0;
+  x0 = sw ? x1 : x0;
+  c1 = sw ? tc : c1;
+  x1 = sw ? tx : x1;
 }
 
-// Sorts the first n_pad (a power of two, >= kIPT) records by (code, idx):
-// sorted runs of 16 per thread in registers, then merge-path merges.
-__device__ void block_merge_sort(FinalSmem& S, int n_pad) {
-  const int active = n_pad / kIPT;
+// Bitonic sort of the first n records by (code, idx), padded to N =
+// kK3Threads * IPT with (~0, ~0) sentinels (they sort last).  Thread t holds
+// sorted positions t*IPT .. t*IPT+IPT-1 in registers.  A stage with partner
+// distance j < IPT runs in registers, IPT <= j < 32*IPT by warp shuffles, and
+// j >= 32*IPT through shared memory in a slot-major layout (item k of thread t
+// at k*kK3Threads + t), which is free of bank conflicts.  No address depends on
+// the data.
+template <int IPT>
+__device__ void bitonic_block_sort(FinalSmem& S, int n) {
+  constexpr int N = kK3Threads * IPT;
   const int t = threadIdx.x;
-  uint64_t c[kIPT];
-  uint32_t x[kIPT];
-  if (t < active) {
+  uint64_t c[IPT];
+  uint32_t x[IPT];
 #pragma unroll
-    for (int k = 0; k < kIPT; ++k) {
-      c[k] = S.code[pidx(t * kIPT + k)];
-      x[k] = S.idx[pidx(t * kIPT + k)];
-    }
-    reg_sort16(c, x);
-#pragma unroll
-    for (int k = 0; k < kIPT; ++k) {
-      S.code[pidx(t * kIPT + k)] = c[k];
-      S.idx[pidx(t * kIPT + k)] = x[k];
-    }
+  for (int k = 0; k < IPT; ++k) {
+    const int i = t * IPT + k;
+    c[k] = i < n ? S.code[pidx(i)] : ~0ull;
+    x[k] = i < n ? S.idx[pidx(i)] : ~0u;
   }
   __syncthreads();
-  for (int R = kIPT; R < n_pad; R <<= 1) {
-    if (t < active) {
-      const int pos = t * kIPT;
-      const int base = pos & ~(2 * R - 1);
-      const int diag = pos - base;
-      int lo = max(0, diag - R), hi = min(diag, R);
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        const int ai = pidx(base + mid), bi = pidx(base + R + diag - 1 - mid);
-        if (!rec_less(S.code[bi], S.idx[bi], S.code[ai], S.idx[ai])) lo = mid + 1;
-        else hi = mid;
-      }
-      int ia = base + lo, ib = base + R + (diag - lo);
-      const int ea = base + R, eb = base + 2 * R;
-      uint64_t ca = ia < ea ? S.code[pidx(ia)] : 0ull;
-      uint32_t xa = ia < ea ? S.idx[pidx(ia)] : 0u;
-      uint64_t cb = ib < eb ? S.code[pidx(ib)] : 0ull;
-      uint32_t xb = ib < eb ? S.idx[pidx(ib)] : 0u;
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int j = size >> 1; j >= IPT; j >>= 1) {
+      const int m = j / IPT;  // partner thread t ^ m
+      const bool keep_min = ((t & m) == 0) == ((t * IPT & size) == 0);
+      if (m < 32) {
 #pragma unroll
-      for (int k = 0; k < kIPT; ++k) {
-        const bool take_a = ia < ea && (ib >= eb || !rec_less(cb, xb, ca, xa));
-        c[k] = take_a ? ca : cb;
-        x[k] = take_a ? xa : xb;
-        if (take_a) {
-          ++ia;
-          if (ia < ea) {
-            ca = S.code[pidx(ia)];
-            xa = S.idx[pidx(ia)];
+        for (int k = 0; k < IPT; ++k) {
+          const uint64_t oc = __shfl_xor_sync(0xffffffffu, c[k], m);
+          const uint32_t ox = __shfl_xor_sync(0xffffffffu, x[k], m);
+          const bool other_less = rec_less(oc, ox, c[k], x[k]);
+          if (other_less == keep_min) {
+            c[k] = oc;
+            x[k] = ox;
           }
-        } else {
-          ++ib;
-          if (ib < eb) {
-            cb = S.code[pidx(ib)];
-            xb = S.idx[pidx(ib)];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          S.code[k * kK3Threads + t] = c[k];
+          S.idx[k * kK3Threads + t] = x[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          const uint64_t oc = S.code[k * kK3Threads + (t ^ m)];
+          const uint32_t ox = S.idx[k * kK3Threads + (t ^ m)];
+          const bool other_less = rec_less(oc, ox, c[k], x[k]);
+          if (other_less == keep_min) {
+            c[k] = oc;
+            x[k] = ox;
           }
+        }
+        __syncthreads();
+      }
+    }
+#pragma unroll
+    for (int jj = IPT / 2; jj > 0; jj >>= 1) {
+      if (jj < size) {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          if ((k & jj) == 0) cas(c[k], x[k], c[k | jj], x[k | jj], ((t * IPT + k) & size) == 0);
         }
       }
     }
-    __syncthreads();
-    if (t < active) {
-#pragma unroll
-      for (int k = 0; k < kIPT; ++k) {
-        S.code[pidx(t * kIPT + k)] = c[k];
-        S.idx[pidx(t * kIPT + k)] = x[k];
-      }
-    }
-    __syncthreads();
   }
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    S.code[pidx(t * IPT + k)] = c[k];
+    S.idx[pidx(t * IPT + k)] = x[k];
+  }
+  __syncthreads();
+}
+
+// Sorts the first n (<= kCap) records by (code, idx) with the narrowest
+// bitonic network that holds them.
+__device__ __forceinline__ void block_sort(FinalSmem& S, int n) {
+  if (n <= kK3Threads) bitonic_block_sort<1>(S, n);
+  else if (n <= 2 * kK3Threads) bitonic_block_sort<2>(S, n);
+  else if (n <= 4 * kK3Threads) bitonic_block_sort<4>(S, n);
+  else bitonic_block_sort<8>(S, n);
 }
 
 // Insertion sort of sorted positions [i, e) by (code, idx); the run is short,
@@ -944,20 +948,6 @@ __device__ void resolve_tie(const Src& src, FinalSmem& S, int i, int e, int L, u
   }
 }
 
-// Left-to-right sum of the coefficients of sorted positions [i, e); flags any
-// coefficient of infinite magnitude.
-template <int KW, class Src>
-__device__ __forceinline__ c128 segment_sum(const Src& src, const FinalSmem& S, int i, int e, bool& inf) {
-  c128 acc{0.0, 0.0};
-  for (int m = i; m < e; ++m) {
-    uint64_t k[KW];
-    const c128 c = src.key_coeff(S.idx[pidx(m)], k);
-    if (!(fabs(c.re) <= 0x1p1022 && fabs(c.im) <= 0x1p1022) && isinf(wgd::hypot_ref(c.re, c.im))) inf = true;
-    acc = wgd::cadd(acc, c);
-  }
-  return acc;
-}
-
 static_assert(kK3Threads == 256, "radix_sort_u32 maps one thread per digit");
 static_assert(sizeof(unsigned) * (256 + (kK3Threads / 32) * 256 + 2) <= sizeof(uint64_t) * kPadded,
               "radix_sort_u32 scratch must fit in the code area");
@@ -1047,16 +1037,15 @@ __device__ const uint32_t* radix_sort_u32(FinalSmem& S, uint32_t* a, uint32_t* t
 }
 
 template <int KW, class Src>
-__global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, FinalParams P) {
+__global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src src, FinalParams P) {
   extern __shared__ __align__(16) unsigned char k3raw[];
   FinalSmem& S = *reinterpret_cast<FinalSmem*>(k3raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const unsigned G = P.ctl->fine_total;
   const double thr = P.ctl->thr;
   bool inf = false;
-  long long tp[5] = {0, 0, 0, 0, 0};
   while (true) {
-    if (P.trace && tid == 0) tp[0] = clock64();
+    if (P.trace && tid == 0) S.tp[0] = clock64();
     if (tid == 0) S.job = atomicAdd(&P.ctl->k3_ticket, 1u);
     __syncthreads();
     const unsigned g = S.job;
@@ -1066,8 +1055,20 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
     const uint32_t cw = P.fine_count[g];
     const int n = static_cast<int>(cw & kCountMask);
     const bool exact = (cw & kExactBit) != 0;
-    const bool pure = (cw & kPureBit) != 0;
+    bool pure = (cw & kPureBit) != 0;
     const bool fits = n <= kCap;
+    if (!fits && !pure) {
+      // an isolated code whose eight digits do not fix the key: one key if
+      // every item's key equals the first
+      uint64_t k0[KW], k[KW];
+      src.key(P.rec_idx[start], k0);
+      bool same = true;
+      for (int i = tid; i < n && same; i += kK3Threads) {
+        src.key(P.rec_idx[start + i], k);
+        same = keq<KW>(k, k0);
+      }
+      pure = __syncthreads_and(same) != 0;
+    }
     if (tid == 0 && n > 0) {
       if (!fits && !pure) atomicOr(&P.ctl->flags, kFlagFineFull);
       atomicMax(&P.ctl->max_fine, static_cast<unsigned>(n));
@@ -1087,19 +1088,18 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
           acc = wgd::cadd(acc, c);
         }
         const bool kp = wgd::hypot_ref(acc.re, acc.im) > thr;
-        P.rec_idx[start] = sorted[0];
-        P.big_sum[2 * g] = acc.re;
-        P.big_sum[2 * g + 1] = acc.im;
+        const uint32_t first = sorted[0];
+        P.rec_idx[start] = first;
+        P.rec_code[start] = static_cast<uint64_t>(__double_as_longlong(acc.re));
+        P.rec_im[start] = acc.im;
         P.counts[g] = kp ? 1u : 0u;
       }
       __syncthreads();
     }
     if (fits && n > 0) {
-      int n_pad = kIPT;
-      while (n_pad < n) n_pad <<= 1;
-      for (int i = tid; i < n_pad; i += kK3Threads) {
-        S.code[pidx(i)] = i < n ? P.rec_code[start + i] : ~0ull;
-        S.idx[pidx(i)] = i < n ? P.rec_idx[start + i] : ~0u;
+      for (int i = tid; i < n; i += kK3Threads) {
+        S.code[pidx(i)] = P.rec_code[start + i];
+        S.idx[pidx(i)] = P.rec_idx[start + i];
       }
       for (int w = tid; w < kWords; w += kK3Threads) {
         S.head[w] = 0;
@@ -1107,9 +1107,9 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
       }
       if (tid == 0) S.n_runs = 0;
       __syncthreads();
-      if (P.trace && tid == 0) tp[1] = clock64();
-      block_merge_sort(S, n_pad);
-      if (P.trace && tid == 0) tp[2] = clock64();
+      if (P.trace && tid == 0) S.tp[1] = clock64();
+      block_sort(S, n);
+      if (P.trace && tid == 0) S.tp[2] = clock64();
       // segment heads where the code changes
       for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
         const int i = i0 + lane;
@@ -1138,44 +1138,81 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
                           &P.ctl->flags);
       }
       __syncthreads();
-      if (P.trace && tid == 0) tp[3] = clock64();
-      // segment sums and the cull
+      if (P.trace && tid == 0) S.tp[3] = clock64();
+      // every item's coefficient, two items per thread in flight; the code
+      // slots take the real parts
+      for (int i0 = tid; i0 < n; i0 += 2 * kK3Threads) {
+        c128 cv[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int i = i0 + u * kK3Threads;
+          if (i < n) {
+            uint64_t k[KW];
+            cv[u] = src.key_coeff(S.idx[pidx(i)], k);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int i = i0 + u * kK3Threads;
+          if (i < n) {
+            const c128 c = cv[u];
+            if (!(fabs(c.re) <= 0x1p1022 && fabs(c.im) <= 0x1p1022) && isinf(wgd::hypot_ref(c.re, c.im))) inf = true;
+            S.code[pidx(i)] = static_cast<uint64_t>(__double_as_longlong(c.re));
+            S.im[pidx(i)] = c.im;
+          }
+        }
+      }
+      __syncthreads();
+      // segment sums, left to right from zero, and the cull; a head's slot
+      // takes its segment's sum
       for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
         const int i = i0 + lane;
         bool kp = false;
         if (i < n && bit_at(S.head, i)) {
-          const c128 s = segment_sum<KW>(src, S, i, next_set(S.head, i, n), inf);
+          const int e = next_set(S.head, i, n);
+          c128 acc{0.0, 0.0};
+          for (int m = i; m < e; ++m)
+            acc = wgd::cadd(acc, c128{__longlong_as_double(static_cast<long long>(S.code[pidx(m)])), S.im[pidx(m)]});
           // without NaNs the rounded |s| is never below max(|re|, |im|), which
           // decides most sums without the full hypot
-          const bool plain = !isnan(s.re) && !isnan(s.im);
-          kp = (plain && (fabs(s.re) > thr || fabs(s.im) > thr)) || wgd::hypot_ref(s.re, s.im) > thr;
+          const bool plain = !isnan(acc.re) && !isnan(acc.im);
+          kp = (plain && (fabs(acc.re) > thr || fabs(acc.im) > thr)) || wgd::hypot_ref(acc.re, acc.im) > thr;
+          S.code[pidx(i)] = static_cast<uint64_t>(__double_as_longlong(acc.re));
+          S.im[pidx(i)] = acc.im;
         }
         const uint32_t b = __ballot_sync(0xffffffffu, kp);
         if (lane == 0) S.keep[i0 >> 5] = b;
       }
       __syncthreads();
-      // sorted indices, segment heads and survivors go back to global memory
-      // for the output pass
+      // survivors before each keep word (at most kWords = 64: two per lane)
       const int nw = (n + 31) >> 5;
-      for (int i = tid; i < n; i += kK3Threads) P.rec_idx[start + i] = S.idx[pidx(i)];
-      unsigned c = 0;
-      for (int w = tid; w < nw; w += kK3Threads) {
-        P.head_bits[(start >> 5) + w] = S.head[w];
-        P.keep_bits[(start >> 5) + w] = S.keep[w];
-        c += __popc(S.keep[w]);
-      }
+      if (warp == 0) {
+        const int w0 = 2 * lane;
+        const unsigned v0 = w0 < nw ? __popc(S.keep[w0]) : 0u, v1 = w0 + 1 < nw ? __popc(S.keep[w0 + 1]) : 0u;
+        unsigned incl = v0 + v1;
 #pragma unroll
-      for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-      if (lane == 0) S.warp_sum[warp] = c;
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const unsigned ex = incl - v0 - v1;
+        if (w0 < nw) S.wpre[w0] = ex;
+        if (w0 + 1 < nw) S.wpre[w0 + 1] = ex + v0;
+        if (lane == 31) P.counts[g] = incl;
+      }
       __syncthreads();
-      if (tid == 0) {
-        unsigned tsum = 0;
-        for (int w = 0; w < kK3Threads / 32; ++w) tsum += S.warp_sum[w];
-        P.counts[g] = tsum;
+      // survivors compacted at the start of the bucket's records: index, sum
+      for (int i = tid; i < n; i += kK3Threads) {
+        const uint32_t kw = S.keep[i >> 5];
+        if (!((kw >> (i & 31)) & 1u)) continue;
+        const uint32_t r = start + S.wpre[i >> 5] + __popc(kw & ((1u << (i & 31)) - 1u));
+        P.rec_idx[r] = S.idx[pidx(i)];
+        P.rec_code[r] = S.code[pidx(i)];
+        P.rec_im[r] = S.im[pidx(i)];
       }
       if (P.trace && tid == 0) {
-        tp[4] = clock64();
-        for (int q = 0; q < 4; ++q) atomicAdd(&P.ctl->phase[q], static_cast<unsigned long long>(tp[q + 1] - tp[q]));
+        S.tp[4] = clock64();
+        for (int q = 0; q < 4; ++q) atomicAdd(&P.ctl->phase[q], static_cast<unsigned long long>(S.tp[q + 1] - S.tp[q]));
       }
     }
     __syncthreads();
@@ -1187,13 +1224,11 @@ __global__ void __launch_bounds__(kK3Threads) bucket_final_kernel(Src src, Final
 
 struct OutputParams {
   const uint32_t* fine_start;
-  const uint32_t* fine_count;
-  const uint32_t* rec_idx;     // sorted within each fine bucket
-  const uint32_t* head_bits;
-  const uint32_t* keep_bits;
+  const uint32_t* rec_idx;     // survivors' indices at the start of each bucket
+  const uint64_t* rec_re;      // their sums
+  const double* rec_im;
   const uint32_t* offsets;     // [G] exclusive prefix of the survivor counts
   const uint32_t* counts;
-  const double* big_sum;
   const Control* ctl;
   uint64_t* out_x;
   uint64_t* out_z;
@@ -1202,88 +1237,34 @@ struct OutputParams {
   unsigned* flags;
 };
 
-// One CTA per fine bucket: each surviving segment head finds its output rank
-// from the bucket offset and the keep bits before it, sums its segment again
-// (the same additions in the same order) and writes key and coefficient.
+// One warp per fine bucket: its survivors go to consecutive ranks from the
+// bucket's offset, each key rebuilt from its operands.
 template <int KW, class Src>
 __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParams P) {
-  __shared__ uint32_t hw[kWords], kw[kWords], wpre[kWords];
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int lane = threadIdx.x & 31;
   const unsigned G = P.ctl->fine_total;
-  for (unsigned g = blockIdx.x; g < G; g += gridDim.x) {
-    if (P.counts[g] == 0) continue;
+  const unsigned warps = gridDim.x * (blockDim.x >> 5);
+  for (unsigned g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < G; g += warps) {
+    const uint32_t cnt = P.counts[g];
+    if (cnt == 0) continue;
     const uint32_t start = P.fine_start[g];
-    const int n = static_cast<int>(P.fine_count[g] & kCountMask);
-    const size_t base_rank = P.offsets[g];
-    if (n > kCap) {
-      // a bucket of one key above kCap items: its sum was formed in order
-      if (tid == 0) {
-        if (base_rank >= P.out_cap) {
-          atomicOr(P.flags, kFlagOverrun);
-        } else {
-          uint64_t k[KW];
-          src.key(P.rec_idx[start], k);
-#pragma unroll
-          for (int w = 0; w < KW / 2; ++w) {
-            P.out_x[base_rank * (KW / 2) + w] = k[2 * w];
-            P.out_z[base_rank * (KW / 2) + w] = k[2 * w + 1];
-          }
-          P.out_c[2 * base_rank] = P.big_sum[2 * g];
-          P.out_c[2 * base_rank + 1] = P.big_sum[2 * g + 1];
-        }
-      }
+    const size_t base = P.offsets[g];
+    if (base + cnt > P.out_cap) {
+      if (lane == 0) atomicOr(P.flags, kFlagOverrun);
       continue;
     }
-    const int nw = (n + 31) >> 5;
-    for (int w = tid; w < nw; w += blockDim.x) {
-      hw[w] = P.head_bits[(start >> 5) + w];
-      kw[w] = P.keep_bits[(start >> 5) + w];
-    }
-    __syncthreads();
-    if (tid < 32) {
-      // exclusive prefix of survivors per bitmask word (at most 4 words per lane)
-      unsigned v[4], s = 0;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int w = lane * 4 + q;
-        v[q] = w < nw ? __popc(kw[w]) : 0u;
-        s += v[q];
-      }
-      unsigned incl = s;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      unsigned run = incl - s;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int w = lane * 4 + q;
-        if (w < nw) wpre[w] = run;
-        run += v[q];
-      }
-    }
-    __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) {
-      if (!bit_at(kw, i)) continue;
-      const size_t o = base_rank + wpre[i >> 5] + __popc(kw[i >> 5] & ((1u << (i & 31)) - 1u));
-      if (o >= P.out_cap) {
-        atomicOr(P.flags, kFlagOverrun);
-        continue;
-      }
-      const int e = next_set(hw, i, n);
+    for (uint32_t i = lane; i < cnt; i += 32) {
       uint64_t k[KW];
-      c128 acc{0.0, 0.0};
-      for (int m = i; m < e; ++m) acc = wgd::cadd(acc, src.key_coeff(P.rec_idx[start + m], k));  // one key
+      src.key(P.rec_idx[start + i], k);
+      const size_t o = base + i;
 #pragma unroll
       for (int w = 0; w < KW / 2; ++w) {
         P.out_x[o * (KW / 2) + w] = k[2 * w];
         P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
       }
-      P.out_c[2 * o] = acc.re;
-      P.out_c[2 * o + 1] = acc.im;
+      P.out_c[2 * o] = __longlong_as_double(static_cast<long long>(P.rec_re[start + i]));
+      P.out_c[2 * o + 1] = P.rec_im[start + i];
     }
-    __syncthreads();
   }
 }
 
@@ -1361,8 +1342,8 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   const size_t ws_bytes = WS::rounded(sizeof(Control)) + WS::rounded(8 * B1) + WS::rounded(4 * B1) +
                           WS::rounded(4 * region) + WS::rounded(4 * (B1 + 1)) + WS::rounded(4 * B1) +
                           WS::rounded(8 * records) + WS::rounded(4 * records) + 2 * WS::rounded(4 * Gmax) +
-                          WS::rounded(2 * Gmax) + WS::rounded(2 * region) + 2 * WS::rounded(records / 8) +
-                          2 * WS::rounded(4 * Gmax) + WS::rounded(16 * Gmax) + WS::rounded(4);
+                          WS::rounded(2 * Gmax) + WS::rounded(2 * region) + WS::rounded(8 * records) +
+                          2 * WS::rounded(4 * Gmax) + WS::rounded(4);
   WS ws(device, ws_bytes, s);
   Control* dctl = ws.take_as<Control>(1);
   wg::check_cuda(cudaMemsetAsync(dctl, 0, sizeof(Control), s), "clear bucket control");
@@ -1424,16 +1405,13 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   stamp("fine");
 
   // final: sort, reduce and cull each fine bucket; survivors per bucket
-  uint32_t* head_bits = ws.take_as<uint32_t>(records / 32);
-  uint32_t* keep_bits = ws.take_as<uint32_t>(records / 32);
+  double* rec_im = ws.take_as<double>(records);
   uint32_t* counts = ws.take_as<uint32_t>(Gmax);
   uint32_t* offsets = ws.take_as<uint32_t>(Gmax);
-  double* big_sum = ws.take_as<double>(2 * Gmax);
   uint32_t* survivors = ws.take_as<uint32_t>(1);
   wg::check_cuda(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * Gmax, s), "clear survivor counts");
   {
-    const FinalParams fp{fine_start, fine_count, fine_L, rec_code, rec_idx, head_bits, keep_bits, counts, big_sum,
-                         dctl, trace ? 1 : 0};
+    const FinalParams fp{fine_start, fine_count, fine_L, rec_code, rec_idx, rec_im, counts, dctl, trace ? 1 : 0};
     auto* k3 = bucket_final_kernel<KW, Src>;
     set_smem(k3, sizeof(FinalSmem));
     int per_sm = 0;
@@ -1469,7 +1447,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   wg::Scratch ox(sizeof(uint64_t) * W * U, s), oz(sizeof(uint64_t) * W * U, s), oc(sizeof(double) * 2 * U, s);
   stamp("alloc");
   {
-    const OutputParams op{fine_start, fine_count, rec_idx, head_bits, keep_bits, offsets, counts, big_sum, dctl,
+    const OutputParams op{fine_start, rec_idx, rec_code, rec_im, offsets, counts, dctl,
                           ox.as<uint64_t>(), oz.as<uint64_t>(), oc.as<double>(), U, &dctl->flags};
     const unsigned grid = static_cast<unsigned>(props.sm_count * 8);
     WG_TIMED("bucket_output_kernel", s, bucket_output_kernel<KW><<<grid, 256, 0, s>>>(src, op));
