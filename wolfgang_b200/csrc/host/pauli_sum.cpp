@@ -14,9 +14,13 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <unordered_set>
 #include <utility>
 #include <vector>
+
+#include <sys/mman.h>
+#include <unistd.h>
 
 #include "abi.hpp"
 #include "guards.hpp"
@@ -34,6 +38,59 @@ void set_bit(std::vector<std::uint64_t>& v, std::size_t words, std::size_t term,
 }
 
 char letter(bool xb, bool zb) { return xb ? (zb ? 'Y' : 'X') : (zb ? 'Z' : 'I'); }
+
+// Result vectors of a large download.  A value-initialised std::vector of
+// many gigabytes spends most of its construction taking 4 KiB page faults one
+// at a time.  Here the storage is reserved first, advised for transparent huge
+// pages and pre-faulted by several threads (MADV_POPULATE_WRITE over disjoint
+// ranges), and the vectors are then value-initialised concurrently over
+// resident memory.  Small results take the plain path.
+constexpr std::size_t kBigHostBytes = std::size_t{64} << 20;
+
+void prefault(void* p, std::size_t bytes, unsigned threads) {
+  const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
+  const std::uintptr_t lo = (reinterpret_cast<std::uintptr_t>(p) + page - 1) & ~(page - 1);
+  const std::uintptr_t hi = (reinterpret_cast<std::uintptr_t>(p) + bytes) & ~(page - 1);
+  if (hi <= lo) return;
+#ifdef MADV_HUGEPAGE
+  madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only: failures are harmless
+#endif
+#ifdef MADV_POPULATE_WRITE
+  const std::size_t span = hi - lo, step = ((span / threads) + page - 1) & ~(page - 1);
+  std::vector<std::thread> pool;
+  for (std::uintptr_t a = lo; a < hi; a += step) {
+    const std::size_t len = std::min<std::size_t>(step, hi - a);
+    pool.emplace_back([a, len] { madvise(reinterpret_cast<void*>(a), len, MADV_POPULATE_WRITE); });
+  }
+  for (auto& t : pool) t.join();
+#endif
+}
+
+void make_result_vectors(std::size_t words_total, std::size_t terms, std::vector<std::uint64_t>& x,
+                         std::vector<std::uint64_t>& z, std::vector<std::complex<double>>& c) {
+  if (16 * words_total + 16 * terms < kBigHostBytes) {
+    x.resize(words_total);
+    z.resize(words_total);
+    c.resize(terms);
+    return;
+  }
+  x.reserve(words_total);
+  z.reserve(words_total);
+  c.reserve(terms);
+  const unsigned hw = std::max(3u, std::min(16u, std::thread::hardware_concurrency()));
+  {
+    std::thread tx([&] { prefault(x.data(), 8 * words_total, hw / 3); });
+    std::thread tz([&] { prefault(z.data(), 8 * words_total, hw / 3); });
+    prefault(c.data(), 16 * terms, hw / 3);
+    tx.join();
+    tz.join();
+  }
+  std::thread tx([&] { x.resize(words_total); });
+  std::thread tz([&] { z.resize(words_total); });
+  c.resize(terms);
+  tx.join();
+  tz.join();
+}
 
 // Operands of one compute call, resident on the compute device.
 struct DeviceOperand {
@@ -238,8 +295,9 @@ PauliSum PauliSum::download_device_result(std::size_t n, std::size_t words, int 
   DeviceBuffer bz = DeviceBuffer::adopt(device, oz, U * words * 8);
   DeviceBuffer bc = DeviceBuffer::adopt(device, oc, U * 16);
   if (U == 0) return PauliSum::empty(n);
-  std::vector<std::uint64_t> x(U * words), z(U * words);
-  std::vector<std::complex<double>> c(U);
+  std::vector<std::uint64_t> x, z;
+  std::vector<std::complex<double>> c;
+  make_result_vectors(U * words, U, x, z, c);
   bx.download(x.data(), x.size() * 8);
   bz.download(z.data(), z.size() * 8);
   bc.download(c.data(), c.size() * 16);
@@ -282,8 +340,9 @@ PauliSum PauliSum::matmul(const PauliSum& rhs, bool simplify_output, std::size_t
     DeviceBuffer bx = DeviceBuffer::adopt(dev, ox, U * words_ * 8);
     DeviceBuffer bz = DeviceBuffer::adopt(dev, oz, U * words_ * 8);
     DeviceBuffer bc = DeviceBuffer::adopt(dev, oc, U * 16);
-    std::vector<std::uint64_t> x(U * words_), z(U * words_);
-    std::vector<std::complex<double>> c(U);
+    std::vector<std::uint64_t> x, z;
+    std::vector<std::complex<double>> c;
+    make_result_vectors(U * words_, U, x, z, c);
     bx.download(x.data(), x.size() * 8);
     bz.download(z.data(), z.size() * 8);
     bc.download(c.data(), c.size() * 16);

@@ -102,6 +102,7 @@ struct Control {
   unsigned max_fine;             // largest fine bucket
   unsigned long long tie_items;  // items in runs of equal 8-digit codes (traced runs)
   unsigned long long phase[4];   // final-kernel cycles per phase (traced runs)
+  unsigned long long fphase[5];  // fine-kernel cycles per phase (traced runs)
 };
 
 // ------------------------------------------------------------------ keys and codes
@@ -554,6 +555,7 @@ struct FineParams {
   uint32_t* fine_count;       // [G] count | kExactBit | kPureBit
   uint16_t* fine_L;           // [G] prefix of the bucket's codes
   Control* ctl;
+  int trace;                  // record per-phase cycles
 };
 
 constexpr size_t kK2Smem = sizeof(uint64_t) * (kSample2 + kFineSlots) + sizeof(int) * kFineSlots +
@@ -588,8 +590,10 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
   __shared__ unsigned s_job;
   __shared__ int s_ns;
   __shared__ unsigned warp_tmp[33];
+  __shared__ long long s_tp[6];
   const int total = P.total;
   while (true) {
+    if (P.trace && threadIdx.x == 0) s_tp[0] = clock64();
     if (threadIdx.x == 0) s_job = atomicAdd(&P.ctl->k2_ticket, 1u);
     __syncthreads();
     const int j = static_cast<int>(s_job);
@@ -621,6 +625,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     }
     __syncthreads();
     smem_bitonic_u64(samp, SP);
+    if (P.trace && threadIdx.x == 0) s_tp[1] = clock64();
     // Splitters, greedily: a bucket closes after the run of equal codes that
     // brings it to its share of the sample; a code whose sample run stands for
     // a quarter of kCap items or more (a heavily repeated key) gets a bucket of
@@ -647,6 +652,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
         i += r;
       }
       s_ns = ns;
+      if (P.trace) s_tp[2] = clock64();
     }
     __syncthreads();
     const int ns = s_ns;
@@ -671,6 +677,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       warp_aggregated_add(cnt, static_cast<unsigned>(f), valid);
     }
     __syncthreads();
+    if (P.trace && threadIdx.x == 0) s_tp[3] = clock64();
     // fine bucket offsets, each bucket starting on a multiple of 32 records
     // (slots <= kFineSlots: a few rounds of the block scan)
     unsigned carry = 0;
@@ -691,6 +698,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       carry += tot;
     }
     __syncthreads();
+    if (P.trace && threadIdx.x == 0) s_tp[4] = clock64();
     // pass 2: (code relative to the fine prefix, index) into fine-bucket order
     for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
       const uint32_t t = t0 + threadIdx.x;
@@ -707,6 +715,10 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       }
     }
     __syncthreads();
+    if (P.trace && threadIdx.x == 0) {
+      s_tp[5] = clock64();
+      for (int q = 0; q < 5; ++q) atomicAdd(&P.ctl->fphase[q], static_cast<unsigned long long>(s_tp[q + 1] - s_tp[q]));
+    }
   }
 }
 
@@ -1392,7 +1404,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   {
     uint16_t* fid_tmp = ws.take_as<uint16_t>(region);
     const FineParams fp{fill, capc, B1, total, fine_base, Lj, idx1, fid_tmp, rstride, rec_code, rec_idx,
-                        fine_start, fine_count, fine_L, dctl};
+                        fine_start, fine_count, fine_L, dctl, trace ? 1 : 0};
     auto* k2 = bucket_fine_kernel<KW, Src>;
     set_smem(k2, kK2Smem);
     int per_sm = 0;
@@ -1435,6 +1447,9 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
                  h.fine_total, h.max_fine, h.flags, U32, h.tie_items);
     std::fprintf(stderr, "bucket final phases (Gcycles, all CTAs): load %.2f sort %.2f ties %.2f sums %.2f\n",
                  h.phase[0] * 1e-9, h.phase[1] * 1e-9, h.phase[2] * 1e-9, h.phase[3] * 1e-9);
+    std::fprintf(stderr,
+                 "bucket fine phases (Gcycles, all CTAs): sample %.2f splitters %.2f count %.2f scan %.2f place %.2f\n",
+                 h.fphase[0] * 1e-9, h.fphase[1] * 1e-9, h.fphase[2] * 1e-9, h.fphase[3] * 1e-9, h.fphase[4] * 1e-9);
   }
   if (h.flags & kFallbackMask) return false;
   size_t U = U32;
