@@ -47,6 +47,8 @@
 
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -558,6 +560,70 @@ struct FineParams {
   int trace;                  // record per-phase cycles
 };
 
+// Exclusive block scans (blockDim.x a multiple of 32, at most 1024; tmp holds
+// 32 ints): the maximum over lower threads (INT_MIN for none) and the minimum
+// over higher threads (INT_MAX for none).
+__device__ int block_prefix_max_excl(int v, int* tmp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x = max(x, y);
+  }
+  if (lane == 31) tmp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < nw ? tmp[lane] : INT_MIN;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w = max(w, y);
+    }
+    int ex = __shfl_up_sync(0xffffffffu, w, 1);
+    if (lane == 0) ex = INT_MIN;
+    if (lane < nw) tmp[lane] = ex;
+  }
+  __syncthreads();
+  int in_warp = __shfl_up_sync(0xffffffffu, x, 1);
+  if (lane == 0) in_warp = INT_MIN;
+  const int r = max(tmp[warp], in_warp);
+  __syncthreads();
+  return r;
+}
+
+__device__ int block_suffix_min_excl(int v, int* tmp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_down_sync(0xffffffffu, x, o);
+    if (lane + o < 32) x = min(x, y);
+  }
+  if (lane == 0) tmp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < nw ? tmp[lane] : INT_MAX;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_down_sync(0xffffffffu, w, o);
+      if (lane + o < 32) w = min(w, y);
+    }
+    int ex = __shfl_down_sync(0xffffffffu, w, 1);
+    if (lane == 31) ex = INT_MAX;
+    if (lane < nw) tmp[lane] = ex;
+  }
+  __syncthreads();
+  int in_warp = __shfl_down_sync(0xffffffffu, x, 1);
+  if (lane == 31) in_warp = INT_MAX;
+  const int r = min(tmp[warp], in_warp);
+  __syncthreads();
+  return r;
+}
+
+constexpr int kPickChunk = kSample2 / kK2Threads;  // sorted samples per thread in the splitter pick
+static_assert(kPickChunk * kK2Threads == kSample2 && kPickChunk <= 31, "splitter pick chunks");
+
 constexpr size_t kK2Smem = sizeof(uint64_t) * (kSample2 + kFineSlots) + sizeof(int) * kFineSlots +
                            sizeof(unsigned) * kFineSlots;
 
@@ -590,6 +656,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
   __shared__ unsigned s_job;
   __shared__ int s_ns;
   __shared__ unsigned warp_tmp[33];
+  __shared__ int s_scan[32];
   __shared__ long long s_tp[6];
   const int total = P.total;
   while (true) {
@@ -626,33 +693,87 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     __syncthreads();
     smem_bitonic_u64(samp, SP);
     if (P.trace && threadIdx.x == 0) s_tp[1] = clock64();
-    // Splitters, greedily: a bucket closes after the run of equal codes that
-    // brings it to its share of the sample; a code whose sample run stands for
-    // a quarter of kCap items or more (a heavily repeated key) gets a bucket of
-    // its own, [c, c + 1).
-    if (threadIdx.x == 0) {
+    // Splitters.  Runs of equal codes in the sorted sample are never cut.  A
+    // bucket boundary goes at the first run that starts in each window of
+    // `share` samples; a code whose sample run stands for a quarter of kCap
+    // items or more (a heavily repeated key) gets a bucket of its own,
+    // [c, c + 1).  Every thread takes kPickChunk consecutive samples; scans
+    // find the run starts around each chunk and the output positions.
+    {
       const int share = max(1, S2 / target);
-      int ns = 0, acc = 0, i = 0;
-      while (i < S2 && ns < slots - 1) {
-        const uint64_t v = samp[i];
-        int r = 1;
-        while (i + r < S2 && samp[i + r] == v) ++r;
-        const bool heavy = r >= kHeavyRun && static_cast<uint64_t>(r) * n >= static_cast<uint64_t>(kCap / 4) * S2;
-        if (heavy && v != ~0ull && ns + 2 <= slots - 1) {
-          if (acc > 0 && (ns == 0 || fs[ns - 1] < v)) fs[ns++] = v;
-          fs[ns++] = v + 1;
-          acc = 0;
-        } else {
-          acc += r;
-          if (acc >= share && i + r < S2) {
-            fs[ns++] = samp[i + r];
-            acc = 0;
-          }
+      const int t = threadIdx.x;
+      uint32_t rs = 0;
+      int first_rs = INT_MAX, last_rs = -1;
+#pragma unroll
+      for (int k = 0; k < kPickChunk; ++k) {
+        const int i = t * kPickChunk + k;
+        if (i < S2 && (i == 0 || samp[i] != samp[i - 1])) {
+          rs |= 1u << k;
+          first_rs = min(first_rs, i);
+          last_rs = i;
         }
-        i += r;
       }
-      s_ns = ns;
-      if (P.trace) s_tp[2] = clock64();
+      const int prev_in = block_prefix_max_excl(last_rs, s_scan);
+      const int next_in = min(block_suffix_min_excl(first_rs, s_scan), S2);
+      // splitters this thread emits: pass 0 counts them, pass 1 writes them
+      unsigned cnt = 0, off = 0, total = 0;
+      for (int pass = 0; pass < 2; ++pass) {
+        int prev = prev_in;
+        unsigned o = off;
+#pragma unroll
+        for (int k = 0; k < kPickChunk; ++k) {
+          if (!((rs >> k) & 1u)) continue;
+          const int i = t * kPickChunk + k;
+          const uint32_t later = rs & ~((2u << k) - 1u);
+          const int r = (later ? t * kPickChunk + __ffs(later) - 1 : next_in) - i;
+          const uint64_t v = samp[i];
+          const bool heavy =
+              r >= kHeavyRun && static_cast<uint64_t>(r) * n >= static_cast<uint64_t>(kCap / 4) * S2 && v != ~0ull;
+          const bool regular = i > 0 && (i / share) != (prev / share);
+          if (pass == 0) {
+            cnt += heavy ? (i > 0 ? 2u : 1u) : (regular ? 1u : 0u);
+          } else {
+            if ((heavy && i > 0) || (!heavy && regular)) fs[o++] = v;
+            if (heavy) fs[o++] = v + 1;
+          }
+          prev = i;
+        }
+        if (pass == 0) {
+          off = block_exclusive_scan(cnt, warp_tmp, &total);
+          if (total > static_cast<unsigned>(slots - 1)) break;  // uniform: the greedy pick below instead
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        if (total <= static_cast<unsigned>(slots - 1)) {
+          s_ns = static_cast<int>(total);
+        } else {
+          // greedy, one thread: a bucket closes after the run that brings it
+          // to its share; heavy runs isolated while slots remain
+          int ns = 0, acc = 0, i = 0;
+          while (i < S2 && ns < slots - 1) {
+            const uint64_t v = samp[i];
+            int r = 1;
+            while (i + r < S2 && samp[i + r] == v) ++r;
+            const bool heavy =
+                r >= kHeavyRun && static_cast<uint64_t>(r) * n >= static_cast<uint64_t>(kCap / 4) * S2;
+            if (heavy && v != ~0ull && ns + 2 <= slots - 1) {
+              if (acc > 0 && (ns == 0 || fs[ns - 1] < v)) fs[ns++] = v;
+              fs[ns++] = v + 1;
+              acc = 0;
+            } else {
+              acc += r;
+              if (acc >= share && i + r < S2) {
+                fs[ns++] = samp[i + r];
+                acc = 0;
+              }
+            }
+            i += r;
+          }
+          s_ns = ns;
+        }
+        if (P.trace) s_tp[2] = clock64();
+      }
     }
     __syncthreads();
     const int ns = s_ns;
