@@ -892,100 +892,6 @@ __device__ __forceinline__ int next_set(const uint32_t* m, int i, int n) {
   return min(n, (w << 5) + __ffs(v) - 1);
 }
 
-// Compare-exchange of a pair of records: (c0, x0) takes the smaller when up,
-// the larger otherwise.
-__device__ __forceinline__ void cas(uint64_t& c0, uint32_t& x0, uint64_t& c1, uint32_t& x1, bool up) {
-  const bool sw = up == rec_less(c1, x1, c0, x0);
-  const uint64_t tc = c0;
-  const uint32_t tx = x0;
-  c0 = sw ? c1 : c0;
-  x0 = sw ? x1 : x0;
-  c1 = sw ? tc : c1;
-  x1 = sw ? tx : x1;
-}
-
-// Bitonic sort of the first n records by (code, idx), padded to N =
-// kK3Threads * IPT with (~0, ~0) sentinels (they sort last).  Thread t holds
-// sorted positions t*IPT .. t*IPT+IPT-1 in registers.  A stage with partner
-// distance j < IPT runs in registers, IPT <= j < 32*IPT by warp shuffles, and
-// j >= 32*IPT through shared memory in a slot-major layout (item k of thread t
-// at k*kK3Threads + t), which is free of bank conflicts.  No address depends on
-// the data.
-template <int IPT>
-__device__ void bitonic_block_sort(FinalSmem& S, int n) {
-  constexpr int N = kK3Threads * IPT;
-  const int t = threadIdx.x;
-  uint64_t c[IPT];
-  uint32_t x[IPT];
-#pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    const int i = t * IPT + k;
-    c[k] = i < n ? S.code[pidx(i)] : ~0ull;
-    x[k] = i < n ? S.idx[pidx(i)] : ~0u;
-  }
-  __syncthreads();
-  for (int size = 2; size <= N; size <<= 1) {
-    for (int j = size >> 1; j >= IPT; j >>= 1) {
-      const int m = j / IPT;  // partner thread t ^ m
-      const bool keep_min = ((t & m) == 0) == ((t * IPT & size) == 0);
-      if (m < 32) {
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-          const uint64_t oc = __shfl_xor_sync(0xffffffffu, c[k], m);
-          const uint32_t ox = __shfl_xor_sync(0xffffffffu, x[k], m);
-          const bool other_less = rec_less(oc, ox, c[k], x[k]);
-          if (other_less == keep_min) {
-            c[k] = oc;
-            x[k] = ox;
-          }
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-          S.code[k * kK3Threads + t] = c[k];
-          S.idx[k * kK3Threads + t] = x[k];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-          const uint64_t oc = S.code[k * kK3Threads + (t ^ m)];
-          const uint32_t ox = S.idx[k * kK3Threads + (t ^ m)];
-          const bool other_less = rec_less(oc, ox, c[k], x[k]);
-          if (other_less == keep_min) {
-            c[k] = oc;
-            x[k] = ox;
-          }
-        }
-        __syncthreads();
-      }
-    }
-#pragma unroll
-    for (int jj = IPT / 2; jj > 0; jj >>= 1) {
-      if (jj < size) {
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-          if ((k & jj) == 0) cas(c[k], x[k], c[k | jj], x[k | jj], ((t * IPT + k) & size) == 0);
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    S.code[pidx(t * IPT + k)] = c[k];
-    S.idx[pidx(t * IPT + k)] = x[k];
-  }
-  __syncthreads();
-}
-
-// Sorts the first n (<= kCap) records by (code, idx) with the narrowest
-// bitonic network that holds them.
-__device__ __forceinline__ void block_sort(FinalSmem& S, int n) {
-  if (n <= kK3Threads) bitonic_block_sort<1>(S, n);
-  else if (n <= 2 * kK3Threads) bitonic_block_sort<2>(S, n);
-  else if (n <= 4 * kK3Threads) bitonic_block_sort<4>(S, n);
-  else bitonic_block_sort<8>(S, n);
-}
-
 // Insertion sort of sorted positions [i, e) by (code, idx); the run is short,
 // or already ordered (then each insertion stops at once).
 __device__ void insertion_sort(FinalSmem& S, int i, int e) {
@@ -1001,6 +907,115 @@ __device__ void insertion_sort(FinalSmem& S, int i, int e) {
     S.code[pidx(r)] = cq;
     S.idx[pidx(r)] = xq;
   }
+}
+
+// Compare-exchange of two sort keys: k0 takes the smaller when up, the larger
+// otherwise.
+__device__ __forceinline__ void cas(uint64_t& k0, uint64_t& k1, bool up) {
+  const bool sw = up == (k1 < k0);
+  const uint64_t t = k0;
+  k0 = sw ? k1 : k0;
+  k1 = sw ? t : k1;
+}
+
+constexpr int kSlotBits = 12;  // slot field of a sort key: positions up to kCap - 1 < 2^12 - 1
+constexpr uint64_t kSlotMask = (uint64_t{1} << kSlotBits) - 1;
+static_assert(kCap < (1 << kSlotBits), "a real sort key must stay below the sentinel");
+
+// Bitonic sort of the first n records by (code, idx).  The network orders one
+// 64-bit key per record: the code with its low kSlotBits bits replaced by the
+// record's position before the sort (keys are distinct, and below the ~0
+// padding).  Records whose codes agree above those bits come out in position
+// order and are put in (code, idx) order afterwards, run by run.  The network
+// is padded to N = kK3Threads * IPT; thread t holds sorted positions t*IPT ..
+// t*IPT+IPT-1 in registers.  A stage with partner distance j < IPT runs in
+// registers, IPT <= j < 32*IPT by warp shuffles, and j >= 32*IPT through shared
+// memory (the im area, unused until the sums) in a slot-major layout (item k of
+// thread t at k*kK3Threads + t), free of bank conflicts.
+template <int IPT>
+__device__ void bitonic_block_sort(FinalSmem& S, int n) {
+  constexpr int N = kK3Threads * IPT;
+  const int t = threadIdx.x;
+  uint64_t* ex = reinterpret_cast<uint64_t*>(S.im);
+  uint64_t key[IPT];
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const int i = t * IPT + k;
+    key[k] = i < n ? (S.code[pidx(i)] & ~kSlotMask) | static_cast<uint64_t>(i) : ~0ull;
+  }
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int j = size >> 1; j >= IPT; j >>= 1) {
+      const int m = j / IPT;  // partner thread t ^ m
+      const bool keep_min = ((t & m) == 0) == ((t * IPT & size) == 0);
+      if (m < 32) {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          const uint64_t o = __shfl_xor_sync(0xffffffffu, key[k], m);
+          if ((o < key[k]) == keep_min) key[k] = o;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) ex[k * kK3Threads + t] = key[k];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          const uint64_t o = ex[k * kK3Threads + (t ^ m)];
+          if ((o < key[k]) == keep_min) key[k] = o;
+        }
+        __syncthreads();
+      }
+    }
+#pragma unroll
+    for (int jj = IPT / 2; jj > 0; jj >>= 1) {
+      if (jj < size) {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          if ((k & jj) == 0) cas(key[k], key[k | jj], ((t * IPT + k) & size) == 0);
+        }
+      }
+    }
+  }
+  // records to their sorted positions: the slots go through shared memory
+  // (the exchange area) so that only one position's record is live at a time
+  uint16_t* slot = reinterpret_cast<uint16_t*>(ex);
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) slot[t * IPT + k] = static_cast<uint16_t>(key[k] & kSlotMask);
+  __syncthreads();
+  uint64_t c[IPT];
+  uint32_t x[IPT];
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const int sl = min(static_cast<int>(slot[t * IPT + k]), n - 1);
+    c[k] = S.code[pidx(sl)];
+    x[k] = S.idx[pidx(sl)];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    if (t * IPT + k < n) {
+      S.code[pidx(t * IPT + k)] = c[k];
+      S.idx[pidx(t * IPT + k)] = x[k];
+    }
+  }
+  __syncthreads();
+  // runs of codes equal above the slot bits: (code, idx) order
+  for (int i = t; i + 1 < n; i += kK3Threads) {
+    const uint64_t hi = S.code[pidx(i)] >> kSlotBits;
+    if ((S.code[pidx(i + 1)] >> kSlotBits) != hi || (i > 0 && (S.code[pidx(i - 1)] >> kSlotBits) == hi)) continue;
+    int e = i + 2;
+    while (e < n && (S.code[pidx(e)] >> kSlotBits) == hi) ++e;
+    insertion_sort(S, i, e);
+  }
+  __syncthreads();
+}
+
+// Sorts the first n (<= kCap) records by (code, idx) with the narrowest
+// bitonic network that holds them.
+__device__ __forceinline__ void block_sort(FinalSmem& S, int n) {
+  if (n <= kK3Threads) bitonic_block_sort<1>(S, n);
+  else if (n <= 2 * kK3Threads) bitonic_block_sort<2>(S, n);
+  else if (n <= 4 * kK3Threads) bitonic_block_sort<4>(S, n);
+  else bitonic_block_sort<8>(S, n);
 }
 
 // Positions [i, e) hold one tie of 16-digit codes: keys with more than 16 set
@@ -1371,9 +1386,11 @@ struct OutputParams {
 };
 
 // One warp per fine bucket: its survivors go to consecutive ranks from the
-// bucket's offset, each key rebuilt from its operands.
+// bucket's offset, each key rebuilt from its operands.  A lane moves four
+// survivors at a time, their loads issued before any store.
 template <int KW, class Src>
 __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParams P) {
+  constexpr int kU = 4;
   const int lane = threadIdx.x & 31;
   const unsigned G = P.ctl->fine_total;
   const unsigned warps = gridDim.x * (blockDim.x >> 5);
@@ -1386,17 +1403,37 @@ __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParam
       if (lane == 0) atomicOr(P.flags, kFlagOverrun);
       continue;
     }
-    for (uint32_t i = lane; i < cnt; i += 32) {
-      uint64_t k[KW];
-      src.key(P.rec_idx[start + i], k);
-      const size_t o = base + i;
+    for (uint32_t i0 = lane; i0 < cnt; i0 += 32 * kU) {
+      uint32_t id[kU];
+      uint64_t re[kU];
+      double im[kU];
 #pragma unroll
-      for (int w = 0; w < KW / 2; ++w) {
-        P.out_x[o * (KW / 2) + w] = k[2 * w];
-        P.out_z[o * (KW / 2) + w] = k[2 * w + 1];
+      for (int u = 0; u < kU; ++u) {
+        const uint32_t i = i0 + 32 * u;
+        if (i < cnt) {
+          id[u] = P.rec_idx[start + i];
+          re[u] = P.rec_re[start + i];
+          im[u] = P.rec_im[start + i];
+        }
       }
-      P.out_c[2 * o] = __longlong_as_double(static_cast<long long>(P.rec_re[start + i]));
-      P.out_c[2 * o + 1] = P.rec_im[start + i];
+      uint64_t k[kU][KW];
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+        if (i0 + 32 * u < cnt) src.key(id[u], k[u]);
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const uint32_t i = i0 + 32 * u;
+        if (i < cnt) {
+          const size_t o = base + i;
+#pragma unroll
+          for (int w = 0; w < KW / 2; ++w) {
+            P.out_x[o * (KW / 2) + w] = k[u][2 * w];
+            P.out_z[o * (KW / 2) + w] = k[u][2 * w + 1];
+          }
+          P.out_c[2 * o] = __longlong_as_double(static_cast<long long>(re[u]));
+          P.out_c[2 * o + 1] = im[u];
+        }
+      }
     }
   }
 }
