@@ -229,48 +229,83 @@ struct FastDiv {
   }
 };
 
+// Operand records: [t][KW + 2] words, the key (x0, z0, x1, z1 in significance
+// order) then the coefficient's re and im bits; KW + 2 is even, so every
+// record starts on 16 bytes and moves as 128-bit loads.
+template <int KW>
+__device__ __forceinline__ void load_key(const uint64_t* rec, uint32_t t, uint64_t (&k)[KW]) {
+  const ulonglong2* r = reinterpret_cast<const ulonglong2*>(rec + static_cast<size_t>(t) * (KW + 2));
+#pragma unroll
+  for (int i = 0; i < KW / 2; ++i) {
+    const ulonglong2 v = __ldg(r + i);
+    k[2 * i] = v.x;
+    k[2 * i + 1] = v.y;
+  }
+}
+
+template <int KW>
+__device__ __forceinline__ c128 load_coeff(const uint64_t* rec, uint32_t t) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(rec + static_cast<size_t>(t) * (KW + 2) + KW));
+  return {v.x, v.y};
+}
+
+// Compressed keys [t][KW] (KW even: 16-byte rows).
+template <int KW>
+__device__ __forceinline__ void load_ckey(const uint64_t* c2, uint32_t t, uint64_t (&k)[KW]) {
+  const ulonglong2* r = reinterpret_cast<const ulonglong2*>(c2 + static_cast<size_t>(t) * KW);
+#pragma unroll
+  for (int i = 0; i < KW / 2; ++i) {
+    const ulonglong2 v = __ldg(r + i);
+    k[2 * i] = v.x;
+    k[2 * i + 1] = v.y;
+  }
+}
+
 // Products p = a*nb + b of two packed operands (rhs acts first).
 template <int KW>
 struct ProdSrc {
-  const uint64_t* ak;  // [na][KW]: x0, z0, x1, z1
-  const uint64_t* bk;  // [nb][KW]
-  const uint64_t* ac2; // [na][KW] compressed keys
-  const uint64_t* bc2; // [nb][KW]
-  const double* ac;
-  const double* bc;
-  const uint8_t* ay;   // popc(x & z) mod 4 of each term
-  const uint8_t* by;
+  const uint64_t* arec;  // [na][KW + 2]
+  const uint64_t* brec;  // [nb][KW + 2]
+  const uint64_t* ac2;   // [na][KW] compressed keys
+  const uint64_t* bc2;   // [nb][KW]
   FastDiv nb;
 
   __device__ __forceinline__ void ckey(uint32_t p, uint64_t (&c)[KW]) const {
     const uint32_t a = nb.div(p), b = p - a * nb.d;
-    const uint64_t* pa = ac2 + static_cast<size_t>(a) * KW;
-    const uint64_t* pb = bc2 + static_cast<size_t>(b) * KW;
+    uint64_t ca[KW], cb[KW];
+    load_ckey<KW>(ac2, a, ca);
+    load_ckey<KW>(bc2, b, cb);
 #pragma unroll
-    for (int i = 0; i < KW; ++i) c[i] = __ldg(pa + i) ^ __ldg(pb + i);
+    for (int i = 0; i < KW; ++i) c[i] = ca[i] ^ cb[i];
   }
   __device__ __forceinline__ void key(uint32_t p, uint64_t (&k)[KW]) const {
     const uint32_t a = nb.div(p), b = p - a * nb.d;
-    const uint64_t* pa = ak + static_cast<size_t>(a) * KW;
-    const uint64_t* pb = bk + static_cast<size_t>(b) * KW;
+    uint64_t ka[KW], kb[KW];
+    load_key<KW>(arec, a, ka);
+    load_key<KW>(brec, b, kb);
 #pragma unroll
-    for (int i = 0; i < KW; ++i) k[i] = __ldg(pa + i) ^ __ldg(pb + i);
+    for (int i = 0; i < KW; ++i) k[i] = ka[i] ^ kb[i];
   }
+  // Key and coefficient of the product: masks XOR'd, phase exponent
+  // e = sum_w [popc(ox&oz) - popc(ax&az) - popc(bx&bz) + 2 popc(ax&bz)] mod 4,
+  // coefficient (ca * cb) * i^e.
   __device__ __forceinline__ c128 key_coeff(uint32_t p, uint64_t (&k)[KW]) const {
     const uint32_t a = nb.div(p), b = p - a * nb.d;
-    const uint64_t* pa = ak + static_cast<size_t>(a) * KW;
-    const uint64_t* pb = bk + static_cast<size_t>(b) * KW;
-    unsigned e = 8u - __ldg(ay + a) - __ldg(by + b);
+    uint64_t ka[KW], kb[KW];
+    load_key<KW>(arec, a, ka);
+    load_key<KW>(brec, b, kb);
+    const c128 ca = load_coeff<KW>(arec, a);
+    const c128 cb = load_coeff<KW>(brec, b);
+    unsigned e = 0, ya = 0, yb = 0;
 #pragma unroll
     for (int i = 0; i < KW; i += 2) {
-      const uint64_t axw = __ldg(pa + i), azw = __ldg(pa + i + 1);
-      const uint64_t bxw = __ldg(pb + i), bzw = __ldg(pb + i + 1);
-      k[i] = axw ^ bxw;
-      k[i + 1] = azw ^ bzw;
-      e += __popcll(k[i] & k[i + 1]) + 2u * __popcll(axw & bzw);
+      k[i] = ka[i] ^ kb[i];
+      k[i + 1] = ka[i + 1] ^ kb[i + 1];
+      e += __popcll(k[i] & k[i + 1]) + 2u * __popcll(ka[i] & kb[i + 1]);
+      ya += __popcll(ka[i] & ka[i + 1]);
+      yb += __popcll(kb[i] & kb[i + 1]);
     }
-    const c128 ca{__ldg(ac + 2 * a), __ldg(ac + 2 * a + 1)};
-    const c128 cb{__ldg(bc + 2 * b), __ldg(bc + 2 * b + 1)};
+    e += 8u - (ya & 3u) - (yb & 3u);
     return wgd::rotate(wgd::cmul(ca, cb), e);
   }
 };
@@ -278,46 +313,37 @@ struct ProdSrc {
 // Input terms of simplify.
 template <int KW>
 struct TermSrc {
-  const uint64_t* tk;  // [n][KW]
-  const uint64_t* tc2; // [n][KW] compressed keys
-  const double* c;
+  const uint64_t* trec;  // [n][KW + 2]
+  const uint64_t* tc2;   // [n][KW] compressed keys
 
-  __device__ __forceinline__ void ckey(uint32_t p, uint64_t (&k)[KW]) const {
-    const uint64_t* pt = tc2 + static_cast<size_t>(p) * KW;
-#pragma unroll
-    for (int i = 0; i < KW; ++i) k[i] = __ldg(pt + i);
-  }
-  __device__ __forceinline__ void key(uint32_t p, uint64_t (&k)[KW]) const {
-    const uint64_t* pt = tk + static_cast<size_t>(p) * KW;
-#pragma unroll
-    for (int i = 0; i < KW; ++i) k[i] = __ldg(pt + i);
-  }
+  __device__ __forceinline__ void ckey(uint32_t p, uint64_t (&k)[KW]) const { load_ckey<KW>(tc2, p, k); }
+  __device__ __forceinline__ void key(uint32_t p, uint64_t (&k)[KW]) const { load_key<KW>(trec, p, k); }
   __device__ __forceinline__ c128 key_coeff(uint32_t p, uint64_t (&k)[KW]) const {
-    key(p, k);
-    return {__ldg(c + 2 * p), __ldg(c + 2 * p + 1)};
+    load_key<KW>(trec, p, k);
+    return load_coeff<KW>(trec, p);
   }
 };
 
 // ------------------------------------------------------------------ packing
 
-// AoS keys [t][2W] in significance order, y = popc(x & z) mod 4, and the OR of
-// every key word into sig.
-__global__ void bucket_pack_kernel(const uint64_t* __restrict__ x, const uint64_t* __restrict__ z, size_t T, int W,
-                                   uint64_t* __restrict__ keys, uint8_t* __restrict__ y,
+// Operand records [t][2W + 2] (key words in significance order, then the
+// coefficient) and the OR of every key word into sig.
+__global__ void bucket_pack_kernel(const uint64_t* __restrict__ x, const uint64_t* __restrict__ z,
+                                   const double* __restrict__ c, size_t T, int W, uint64_t* __restrict__ rec,
                                    unsigned long long* __restrict__ sig) {
   uint64_t acc[4] = {0, 0, 0, 0};
+  const int R = 2 * W + 2;
   for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < T;
        t += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    unsigned yy = 0;
     for (int w = 0; w < W; ++w) {
       const uint64_t xv = x[t * W + w], zv = z[t * W + w];
-      keys[t * 2 * W + 2 * w] = xv;
-      keys[t * 2 * W + 2 * w + 1] = zv;
+      rec[t * R + 2 * w] = xv;
+      rec[t * R + 2 * w + 1] = zv;
       acc[2 * w] |= xv;
       acc[2 * w + 1] |= zv;
-      yy += __popcll(xv & zv);
     }
-    if (y) y[t] = static_cast<uint8_t>(yy & 3u);
+    rec[t * R + 2 * W] = static_cast<uint64_t>(__double_as_longlong(c[2 * t]));
+    rec[t * R + 2 * W + 1] = static_cast<uint64_t>(__double_as_longlong(c[2 * t + 1]));
   }
   for (int i = 0; i < 2 * W; ++i) {
     uint64_t v = acc[i];
@@ -331,15 +357,15 @@ struct SigWords {
   uint64_t w[4];
 };
 
-// Compressed keys [t][KW] of packed keys [t][KW] under the significant bits.
-__global__ void bucket_compress_kernel(const uint64_t* __restrict__ keys, size_t T, int KW, SigWords sig,
+// Compressed keys [t][KW] of the records' keys under the significant bits.
+__global__ void bucket_compress_kernel(const uint64_t* __restrict__ rec, size_t T, int KW, SigWords sig,
                                        uint64_t* __restrict__ out) {
   for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < T;
        t += static_cast<size_t>(gridDim.x) * blockDim.x) {
     uint64_t c[4] = {0, 0, 0, 0};
     int base = 0;
     for (int w = 0; w < KW; ++w) {
-      uint64_t m = keys[t * KW + w] & sig.w[w];
+      uint64_t m = rec[t * (KW + 2) + w] & sig.w[w];
       while (m) {
         const int b = 63 - __clzll(m);
         m ^= uint64_t{1} << b;
@@ -1637,22 +1663,20 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   return true;
 }
 
-// Packs terms to AoS keys (+ y) and ORs their words into sig (device).
-void pack(const uint64_t* x, const uint64_t* z, size_t T, int W, wg::Scratch& keys, wg::Scratch* y,
+// Packs terms to operand records and ORs their key words into sig (device).
+void pack(const uint64_t* x, const uint64_t* z, const double* c, size_t T, int W, wg::Scratch& rec,
           unsigned long long* sig, int device, cudaStream_t s) {
-  keys.reset(sizeof(uint64_t) * 2 * W * std::max<size_t>(T, 1), s);
-  if (y) y->reset(std::max<size_t>(T, 1), s);
+  rec.reset(sizeof(uint64_t) * (2 * W + 2) * std::max<size_t>(T, 1), s);
   WG_TIMED("bucket_pack_kernel", s,
-    bucket_pack_kernel<<<wg::grid_for(T, 256, device, 4), 256, 0, s>>>(x, z, T, W, keys.as<uint64_t>(),
-                                                                        y ? y->as<uint8_t>() : nullptr, sig));
+    bucket_pack_kernel<<<wg::grid_for(T, 256, device, 4), 256, 0, s>>>(x, z, c, T, W, rec.as<uint64_t>(), sig));
   wg::check_launch("launch bucket pack");
 }
 
-void compress(const wg::Scratch& keys, size_t T, int KW, const SigWords& sig, wg::Scratch& out, int device,
+void compress(const wg::Scratch& rec, size_t T, int KW, const SigWords& sig, wg::Scratch& out, int device,
               cudaStream_t s) {
   out.reset(sizeof(uint64_t) * KW * std::max<size_t>(T, 1), s);
   WG_TIMED("bucket_compress_kernel", s,
-    bucket_compress_kernel<<<wg::grid_for(T, 256, device, 4), 256, 0, s>>>(keys.as<uint64_t>(), T, KW, sig,
+    bucket_compress_kernel<<<wg::grid_for(T, 256, device, 4), 256, 0, s>>>(rec.as<uint64_t>(), T, KW, sig,
                                                                             out.as<uint64_t>()));
   wg::check_launch("launch bucket compress");
 }
@@ -1688,9 +1712,9 @@ bool bucket_products(int device, int W, const uint64_t* lx, const uint64_t* lz, 
   const int KW = 2 * W;
   Scratch sig(sizeof(unsigned long long) * 4, s);
   check_cuda(cudaMemsetAsync(sig.get(), 0, sizeof(unsigned long long) * 4, s), "clear significant bits");
-  Scratch ak, bk, ay, by, ac2, bc2;
-  pack(lx, lz, n_l, W, ak, &ay, sig.as<unsigned long long>(), device, s);
-  pack(rx, rz, n_r, W, bk, &by, sig.as<unsigned long long>(), device, s);
+  Scratch ak, bk, ac2, bc2;
+  pack(lx, lz, lc, n_l, W, ak, sig.as<unsigned long long>(), device, s);
+  pack(rx, rz, rc, n_r, W, bk, sig.as<unsigned long long>(), device, s);
   SigWords sw{};
   const int total = read_sig(sig, KW, sw, s);
   if (total < 1 || total > 255) return false;
@@ -1700,12 +1724,10 @@ bool bucket_products(int device, int W, const uint64_t* lx, const uint64_t* lz, 
   const Outs out{ox, oz, oc, U};
   const FastDiv fd{static_cast<uint32_t>(n_r), n_r > 1 ? ~0ull / n_r + 1 : 0ull};
   if (W == 1) {
-    const ProdSrc<2> src{ak.as<uint64_t>(), bk.as<uint64_t>(), ac2.as<uint64_t>(), bc2.as<uint64_t>(),
-                         lc, rc, ay.as<uint8_t>(), by.as<uint8_t>(), fd};
+    const ProdSrc<2> src{ak.as<uint64_t>(), bk.as<uint64_t>(), ac2.as<uint64_t>(), bc2.as<uint64_t>(), fd};
     return run_bucket<2>(device, src, static_cast<uint32_t>(P), total, thr, out, s);
   }
-  const ProdSrc<4> src{ak.as<uint64_t>(), bk.as<uint64_t>(), ac2.as<uint64_t>(), bc2.as<uint64_t>(),
-                       lc, rc, ay.as<uint8_t>(), by.as<uint8_t>(), fd};
+  const ProdSrc<4> src{ak.as<uint64_t>(), bk.as<uint64_t>(), ac2.as<uint64_t>(), bc2.as<uint64_t>(), fd};
   return run_bucket<4>(device, src, static_cast<uint32_t>(P), total, thr, out, s);
 }
 
@@ -1717,7 +1739,7 @@ bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, co
   Scratch sig(sizeof(unsigned long long) * 4, s);
   check_cuda(cudaMemsetAsync(sig.get(), 0, sizeof(unsigned long long) * 4, s), "clear significant bits");
   Scratch tk, tc2;
-  pack(x, z, n, W, tk, nullptr, sig.as<unsigned long long>(), device, s);
+  pack(x, z, c, n, W, tk, sig.as<unsigned long long>(), device, s);
   SigWords sw{};
   const int total = read_sig(sig, KW, sw, s);
   if (total < 1 || total > 255) return false;
@@ -1725,10 +1747,10 @@ bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, co
   const ThrSpec thr{thr_mode, atol, rtol, 0.0};
   const Outs out{ox, oz, oc, U};
   if (W == 1) {
-    const TermSrc<2> src{tk.as<uint64_t>(), tc2.as<uint64_t>(), c};
+    const TermSrc<2> src{tk.as<uint64_t>(), tc2.as<uint64_t>()};
     return run_bucket<2>(device, src, static_cast<uint32_t>(n), total, thr, out, s);
   }
-  const TermSrc<4> src{tk.as<uint64_t>(), tc2.as<uint64_t>(), c};
+  const TermSrc<4> src{tk.as<uint64_t>(), tc2.as<uint64_t>()};
   return run_bucket<4>(device, src, static_cast<uint32_t>(n), total, thr, out, s);
 }
 
