@@ -952,7 +952,7 @@ static_assert(kCap < (1 << kSlotBits), "a real sort key must stay below the sent
 // 64-bit key per record: the code with its low kSlotBits bits replaced by the
 // record's position before the sort (keys are distinct, and below the ~0
 // padding).  Records whose codes agree above those bits come out in position
-// order and are put in (code, idx) order afterwards, run by run.  The network
+// order; the caller puts them in (code, idx) order, run by run.  The network
 // is padded to N = kK3Threads * IPT; thread t holds sorted positions t*IPT ..
 // t*IPT+IPT-1 in registers.  A stage with partner distance j < IPT runs in
 // registers, IPT <= j < 32*IPT by warp shuffles, and j >= 32*IPT through shared
@@ -1022,15 +1022,6 @@ __device__ void bitonic_block_sort(FinalSmem& S, int n) {
       S.code[pidx(t * IPT + k)] = c[k];
       S.idx[pidx(t * IPT + k)] = x[k];
     }
-  }
-  __syncthreads();
-  // runs of codes equal above the slot bits: (code, idx) order
-  for (int i = t; i + 1 < n; i += kK3Threads) {
-    const uint64_t hi = S.code[pidx(i)] >> kSlotBits;
-    if ((S.code[pidx(i + 1)] >> kSlotBits) != hi || (i > 0 && (S.code[pidx(i - 1)] >> kSlotBits) == hi)) continue;
-    int e = i + 2;
-    while (e < n && (S.code[pidx(e)] >> kSlotBits) == hi) ++e;
-    insertion_sort(S, i, e);
   }
   __syncthreads();
 }
@@ -1283,6 +1274,30 @@ __global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src 
       __syncthreads();
       if (P.trace && tid == 0) S.tp[1] = clock64();
       block_sort(S, n);
+      // Runs of codes equal above the slot bits, each handled by the thread at
+      // its first position: (code, idx) order by insertion, and within it the
+      // runs of one position code whose eighth digit is set (the key may have
+      // more set bits) are listed for tie resolution once every thread is done.
+      for (int i = tid; i + 1 < n; i += kK3Threads) {
+        const uint64_t hi = S.code[pidx(i)] >> kSlotBits;
+        if ((S.code[pidx(i + 1)] >> kSlotBits) != hi || (i > 0 && (S.code[pidx(i - 1)] >> kSlotBits) == hi)) continue;
+        int e = i + 2;
+        while (e < n && (S.code[pidx(e)] >> kSlotBits) == hi) ++e;
+        insertion_sort(S, i, e);
+        if (exact) continue;
+        for (int a = i; a < e;) {
+          const uint64_t ca = S.code[pidx(a)];
+          int b = a + 1;
+          while (b < e && S.code[pidx(b)] == ca) ++b;
+          if (b - a > 1 && (ca & 0xffu) != 0) {
+            const unsigned q = atomicAdd(&S.n_runs, 1u);
+            S.runs[q] = (static_cast<uint32_t>(a) << 16) | static_cast<uint32_t>(b);
+            if (P.trace) atomicAdd(&P.ctl->tie_items, static_cast<unsigned long long>(b - a));
+          }
+          a = b;
+        }
+      }
+      __syncthreads();
       if (P.trace && tid == 0) S.tp[2] = clock64();
       // segment heads where the code changes
       for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
@@ -1291,20 +1306,9 @@ __global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src 
         const uint32_t b = __ballot_sync(0xffffffffu, h);
         if (lane == 0) S.head[i0 >> 5] = b;
       }
+      // tie resolution rewrites codes and sets heads: every head word first
+      __syncthreads();
       if (!exact) {
-        // runs of equal position code, listed by the thread at the run's first
-        // position, then resolved once every thread is done reading codes
-        for (int i = tid; i + 1 < n; i += kK3Threads) {
-          const uint64_t ci = S.code[pidx(i)];
-          // a code with an empty eighth digit holds every set bit: one key
-          if ((ci & 0xffu) == 0 || (i > 0 && S.code[pidx(i - 1)] == ci) || S.code[pidx(i + 1)] != ci) continue;
-          int e = i + 2;
-          while (e < n && S.code[pidx(e)] == ci) ++e;
-          const unsigned q = atomicAdd(&S.n_runs, 1u);
-          S.runs[q] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(e);
-          if (P.trace) atomicAdd(&P.ctl->tie_items, static_cast<unsigned long long>(e - i));
-        }
-        __syncthreads();
         const int L = P.fine_L[g];
         const int nr = static_cast<int>(S.n_runs);
         for (int q = tid; q < nr; q += kK3Threads)
@@ -1451,13 +1455,18 @@ __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParam
         const uint32_t i = i0 + 32 * u;
         if (i < cnt) {
           const size_t o = base + i;
+          if (KW == 4) {
+            reinterpret_cast<ulonglong2*>(P.out_x)[o] = make_ulonglong2(k[u][0], k[u][2]);
+            reinterpret_cast<ulonglong2*>(P.out_z)[o] = make_ulonglong2(k[u][1], k[u][3]);
+          } else {
 #pragma unroll
-          for (int w = 0; w < KW / 2; ++w) {
-            P.out_x[o * (KW / 2) + w] = k[u][2 * w];
-            P.out_z[o * (KW / 2) + w] = k[u][2 * w + 1];
+            for (int w = 0; w < KW / 2; ++w) {
+              P.out_x[o * (KW / 2) + w] = k[u][2 * w];
+              P.out_z[o * (KW / 2) + w] = k[u][2 * w + 1];
+            }
           }
-          P.out_c[2 * o] = __longlong_as_double(static_cast<long long>(re[u]));
-          P.out_c[2 * o + 1] = im[u];
+          reinterpret_cast<double2*>(P.out_c)[o] =
+              make_double2(__longlong_as_double(static_cast<long long>(re[u])), im[u]);
         }
       }
     }
@@ -1506,6 +1515,11 @@ template <class K>
 void set_smem(K kernel, size_t bytes) {
   wg::check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
                  "set bucket kernel shared memory");
+  // the occupancy the grids are sized for assumes the largest shared-memory
+  // configuration: ask for it, whatever ran before on the SM
+  wg::check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      static_cast<int>(cudaSharedmemCarveoutMaxShared)),
+                 "set bucket kernel shared-memory carveout");
 }
 
 template <int KW, class Src>
@@ -1614,6 +1628,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
     wg::check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3, kK3Threads, sizeof(FinalSmem)),
                    "query final occupancy");
     const unsigned grid = static_cast<unsigned>(props.sm_count * std::max(1, per_sm));
+    if (trace) std::fprintf(stderr, "bucket final: %d CTAs per SM, %zu bytes of shared memory each\n", per_sm, sizeof(FinalSmem));
     WG_TIMED("bucket_final_kernel", s, k3<<<grid, kK3Threads, sizeof(FinalSmem), s>>>(src, fp));
     wg::check_launch("launch bucket final");
   }
