@@ -259,8 +259,8 @@ def bench_products(args, world, rank, torch) -> dict:
         # operand gathers hit L2 and are not counted
         "bucket_coarse_kernel": P * 4,                         # write the item index
         "bucket_fine_kernel": P * (4 + 2 + 2 + 4 + 8 + 4),     # idx, fine id (w+r), idx, code + idx out
-        "bucket_final_kernel": P * (8 + 4 + 4) + P // 4,       # code + idx in, sorted idx out, bitmasks
-        "bucket_output_kernel": P * 4 + P // 4 + U * (8 * 2 * W + 16),  # idx, bitmasks, the U terms
+        "bucket_final_kernel": P * (8 + 4) + U * (4 + 16),     # code + idx in; survivors' idx + sum out
+        "bucket_output_kernel": U * (4 + 16) + U * (8 * 2 * W + 16),  # survivors in, the U terms out
     }
     peak, peak_kind = peaks()
     out = {
@@ -275,9 +275,9 @@ def bench_products(args, world, rank, torch) -> dict:
                    "survey_bytes_per_step": 2 * P * 48 + U * 48,
                    "survey_effective_GBps": (2 * P * 48 + U * 48) / (ms_per_step * 1e-3) / 1e9},
         # DRAM bytes per item of bucket_final_kernel measured by ncu (read + write,
-        # 524.6 MB for a 33,554,432-product case of this workload)
+        # 1017.1 MB for a 33,554,432-product case of this workload)
         "roofline": roofline(prof, per_launch, peak, peak_kind,
-                             traffic={"bucket_final_kernel": int(P * 524.6e6 / 33554432)}),
+                             traffic={"bucket_final_kernel": int(P * 1017.1e6 / 33554432)}),
         "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
