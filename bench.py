@@ -410,8 +410,24 @@ def bench_expectation(args, world, rank, torch) -> dict:
     rl = roofline(prof, {"expect_forward_kernel": G * psi_bytes,
                          "expect_adjoint_kernel": G * psi_bytes + (1 << n) * 16}, peak, kind)
     del res
+    out_cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # reference expectation_statevector_complex128 (forward only: the
+        # reference has no gradient) on the first k terms, scaled to all T
+        from oracle import Reference
+
+        k = args.cpu_terms
+        hpsi = psi.to(torch.complex128).cpu().numpy()
+        x, z, c = op[1][:k], op[2][:k], op[3][:k]
+        t0 = time.perf_counter()
+        Reference().expectation(n, x, z, c, hpsi)
+        per_term = (time.perf_counter() - t0) / k
+        out_cpu = {"value": 1.0 / (per_term * len(op[3])), "unit": "evals/s", "cores": 1, "kind": "reference",
+                   "sample": f"reference expectation_statevector_complex128 on the first {k} of {len(op[3])} terms "
+                             f"({per_term:.3f} s per term), scaled to all terms; forward only (no gradient in "
+                             f"the reference)"}
     return {"metric": "E+grad evals/s" if not args.forward_only else "E evals/s", "value": world * 1e3 / t,
-            "unit": "evals/s", "ms_per_step": t,
+            "unit": "evals/s", "ms_per_step": t, "cpu_baseline": out_cpu,
             "config": {"workload": f"config4: {n} qubits, {len(op[3])} terms, {G} x-groups, "
                                    f"{'c64' if args.c64 else 'c128'} psi, forward{'' if args.forward_only else '+adjoint'}",
                        "survey_bytes_per_step": G * psi_bytes + (0 if args.forward_only else 2 * psi_bytes + G * psi_bytes)},
@@ -448,12 +464,39 @@ def bench_batched(args, world, rank, torch) -> dict:
     pc_total, _, _, _ = timed_steps(torch, max(1, args.steps // 2), 1, per_call)
     pc = pc_total / max(1, args.steps // 2)
     npairs = len(pairs) * world
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # reference expectation (forward only) per term measured at a few qubit
+        # counts on this config's own operators; every pair's time estimated
+        # as T * 2^n * (time per amplitude at the nearest probed size)
+        from oracle import Reference
+
+        from wolfgang_b200.workloads import config5_state
+
+        ref = Reference()
+        probe = {}
+        for n_probe in (12, 16, 20, 24):
+            op = config5_operator(n_probe, 64, 7 + n_probe)
+            st = config5_state(n_probe, 7 + n_probe)
+            k = 64 if n_probe <= 20 else 4
+            t0 = time.perf_counter()
+            ref.expectation(n_probe, op[1][:k], op[2][:k], op[3][:k], st)
+            probe[n_probe] = (time.perf_counter() - t0) / k / (1 << n_probe)
+        def per_amp(n):
+            return probe[min(probe, key=lambda q: abs(q - n))]
+
+        est = sum(T * per_amp(n) * (1 << n) for n, T, _ in pairs)
+        cpu = {"value": len(pairs) / est, "unit": "evals/s", "cores": 1, "kind": "reference",
+               "sample": "reference expectation_statevector_complex128 timed per term at 12/16/20/24 qubits "
+                         f"({', '.join(f'{q}: {v * 1e9:.2f} ns/amp' for q, v in probe.items())}); every pair "
+                         "estimated as T * 2^n * (ns per amplitude at the nearest probed size); forward only (no gradient in the "
+                         f"reference); {est:.0f} s estimated for the batch"}
     return {"metric": "batched E+grad evals/s", "value": npairs / (t * 1e-3), "unit": "evals/s", "ms_per_step": t,
             "config": {"workload": f"config5: {npairs} uneven (H, psi) pairs, n in [8,24], T log-uniform "
                                    f"[100,50000], {'c64' if args.c64 else 'c128'}, forward+gradient, one CUDA graph",
                        "per_call_evals_per_s": len(pairs) / (pc * 1e-3), "per_call_ms": pc,
                        "batched_over_per_call": pc / t},
-            "gpu_launches": launches, "clocks": clocks,
+            "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
 
 
@@ -497,6 +540,7 @@ def main() -> None:
     ap.add_argument("--pairs", type=int, default=512, help="batched pairs (config 5)")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-rows", type=int, default=1024)
+    ap.add_argument("--cpu-terms", type=int, default=8, help="reference terms timed for the expectation baseline")
     ap.add_argument("--ref-rows", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lhs-terms", type=int, default=32768, help="A terms (smaller values: profiling cases)")

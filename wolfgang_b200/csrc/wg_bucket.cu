@@ -1274,28 +1274,14 @@ __global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src 
       __syncthreads();
       if (P.trace && tid == 0) S.tp[1] = clock64();
       block_sort(S, n);
-      // Runs of codes equal above the slot bits, each handled by the thread at
-      // its first position: (code, idx) order by insertion, and within it the
-      // runs of one position code whose eighth digit is set (the key may have
-      // more set bits) are listed for tie resolution once every thread is done.
+      // runs of codes equal above the slot bits, each put in (code, idx) order
+      // by the thread at its first position
       for (int i = tid; i + 1 < n; i += kK3Threads) {
         const uint64_t hi = S.code[pidx(i)] >> kSlotBits;
         if ((S.code[pidx(i + 1)] >> kSlotBits) != hi || (i > 0 && (S.code[pidx(i - 1)] >> kSlotBits) == hi)) continue;
         int e = i + 2;
         while (e < n && (S.code[pidx(e)] >> kSlotBits) == hi) ++e;
         insertion_sort(S, i, e);
-        if (exact) continue;
-        for (int a = i; a < e;) {
-          const uint64_t ca = S.code[pidx(a)];
-          int b = a + 1;
-          while (b < e && S.code[pidx(b)] == ca) ++b;
-          if (b - a > 1 && (ca & 0xffu) != 0) {
-            const unsigned q = atomicAdd(&S.n_runs, 1u);
-            S.runs[q] = (static_cast<uint32_t>(a) << 16) | static_cast<uint32_t>(b);
-            if (P.trace) atomicAdd(&P.ctl->tie_items, static_cast<unsigned long long>(b - a));
-          }
-          a = b;
-        }
       }
       __syncthreads();
       if (P.trace && tid == 0) S.tp[2] = clock64();
@@ -1306,9 +1292,20 @@ __global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src 
         const uint32_t b = __ballot_sync(0xffffffffu, h);
         if (lane == 0) S.head[i0 >> 5] = b;
       }
-      // tie resolution rewrites codes and sets heads: every head word first
-      __syncthreads();
       if (!exact) {
+        // runs of equal position code, listed by the thread at the run's first
+        // position, then resolved once every thread is done reading codes
+        for (int i = tid; i + 1 < n; i += kK3Threads) {
+          const uint64_t ci = S.code[pidx(i)];
+          // a code with an empty eighth digit holds every set bit: one key
+          if ((ci & 0xffu) == 0 || (i > 0 && S.code[pidx(i - 1)] == ci) || S.code[pidx(i + 1)] != ci) continue;
+          int e = i + 2;
+          while (e < n && S.code[pidx(e)] == ci) ++e;
+          const unsigned q = atomicAdd(&S.n_runs, 1u);
+          S.runs[q] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(e);
+          if (P.trace) atomicAdd(&P.ctl->tie_items, static_cast<unsigned long long>(e - i));
+        }
+        __syncthreads();
         const int L = P.fine_L[g];
         const int nr = static_cast<int>(S.n_runs);
         for (int q = tid; q < nr; q += kK3Threads)
