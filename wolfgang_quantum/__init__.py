@@ -19,6 +19,13 @@ from wolfgang_b200 import (  # noqa: F401
     metal_available,
     metal_devices,
 )
+from .openfermion import _install_pauli_sum_openfermion_methods
+from .qiskit import _install_pauli_sum_qiskit_methods
+
+# PauliSum.from_qiskit / to_qiskit / from_openfermion / to_openfermion, as the
+# reference installs them (python/wolfgang_quantum/__init__.py:43-47)
+_install_pauli_sum_qiskit_methods()
+_install_pauli_sum_openfermion_methods()
 
 __all__ = [
     "DeviceCommutationMatrix",
