@@ -382,6 +382,49 @@ def bench_commutation(args, world, rank, torch) -> dict:
     return out
 
 
+def bench_grouping(args, world, rank, torch) -> dict:
+    """Config 3, second half: group_commuting of the 262,144-term operator (mode qwc, or full)."""
+    from wolfgang_b200 import capi
+    from wolfgang_b200.workloads import config3
+
+    n, x, z, c = config3(args.terms)
+    T = len(x)
+    dx, dz = dev(torch, x), dev(torch, z)
+    order = np.zeros(T, np.uintp)
+    sizes = np.zeros(T, np.uintp)
+    psz = ctypes.POINTER(ctypes.c_size_t)
+    ng = ctypes.c_size_t()
+    L = capi.lib()
+    sh = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    full = 1 if args.group_mode == "full" else 0
+
+    def step():
+        capi.check(L.wg_group_commuting(torch.cuda.current_device(), 2, T, dx.data_ptr(), dz.data_ptr(), full,
+                                        order.ctypes.data_as(psz), sizes.ctypes.data_as(psz), ctypes.byref(ng), sh))
+
+    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, step)
+    t = max_over_ranks(total, world) / args.steps
+    out = {"metric": "group_commuting terms/s", "value": world * T / (t * 1e-3), "unit": "terms/s", "ms_per_step": t,
+           "config": {"workload": f"config3: group_commuting(mode={args.group_mode!r}) of {T} terms, 128 qubits, "
+                                  "p=0.05", "groups": int(ng.value)},
+           "roofline": {"bound": "latency", "note": "sequential first-fit: one CTA examines every open group per "
+                                                   "term, terms in the deterministic order"},
+           "gpu_launches": launches, "clocks": clocks,
+           "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import Reference
+
+        rows = min(T, args.cpu_group_terms)
+        t0 = time.perf_counter()
+        groups = Reference().group_commuting(n, x[:rows], z[:rows], c[:rows], mode=args.group_mode)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": rows / dt, "unit": "terms/s", "cores": 1, "kind": "reference",
+                               "sample": f"reference PauliSum::group_commuting(mode={args.group_mode!r}) on the first "
+                                         f"{rows} terms ({len(groups)} groups, {dt:.1f} s); the greedy's cost grows "
+                                         "with the number of open groups, so the full operator runs slower per term"}
+    return out
+
+
 def bench_expectation(args, world, rank, torch) -> dict:
     """Config 4: 26 qubits (1 GiB psi), 20,000 Hermitian terms in 2,000 x-groups; E + dE/dc + dE/dpsi*."""
     from wolfgang_b200.expectation import ExpectationPlan
@@ -531,7 +574,10 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["products", "commutation", "expectation", "batched"], default="products")
+    ap.add_argument("--workload", choices=["products", "commutation", "grouping", "expectation", "batched"],
+                    default="products")
+    ap.add_argument("--group-mode", choices=["qwc", "full"], default="qwc", help="grouping mode (config 3)")
+    ap.add_argument("--cpu-group-terms", type=int, default=16384, help="reference terms timed for grouping")
     ap.add_argument("--terms", type=int, default=262144, help="commutation terms (config 3)")
     ap.add_argument("--algo", type=int, default=0, help="commutation algorithm: 0 auto, 1 ballot, 2 bit-plane")
     ap.add_argument("--qubits", type=int, default=26, help="expectation qubits (config 4)")
@@ -563,11 +609,11 @@ def main() -> None:
 
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    fn = {"products": bench_products, "commutation": bench_commutation, "expectation": bench_expectation,
-          "batched": bench_batched}[args.workload]
+    fn = {"products": bench_products, "commutation": bench_commutation, "grouping": bench_grouping,
+          "expectation": bench_expectation, "batched": bench_batched}[args.workload]
     out = fn(args, world, rank, torch)
     out.update(n_gpus=world, steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling="weak",
-               vs_baseline=None, dtype="u64" if args.workload == "commutation" else "f64",
+               vs_baseline=None, dtype="u64" if args.workload in ("commutation", "grouping") else "f64",
                data=f"synthetic (seeded generator, workload {args.workload})")
     if rank == 0:
         print(json.dumps(out), flush=True)
