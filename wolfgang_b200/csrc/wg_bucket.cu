@@ -203,20 +203,6 @@ __device__ __forceinline__ int upper_bound_u64(const uint64_t* a, int n, uint64_
   return lo;
 }
 
-// Rank of this lane's value among equal values of the warp, via one shared
-// memory atomic per distinct value: returns old counter + rank among peers.
-__device__ __forceinline__ unsigned warp_aggregated_add(unsigned* counters, unsigned key, bool valid) {
-  const unsigned mask = __activemask();
-  const unsigned lane = threadIdx.x & 31;
-  const unsigned k = valid ? key : 0xffffffffu;
-  const unsigned peers = __match_any_sync(mask, k);
-  const int leader = __ffs(peers) - 1;
-  unsigned base = 0;
-  if (valid && static_cast<int>(lane) == leader) base = atomicAdd(&counters[key], __popc(peers));
-  base = __shfl_sync(mask, base, leader);
-  return base + __popc(peers & ((1u << lane) - 1u));
-}
-
 // ------------------------------------------------------------------ item sources
 
 // Exact quotient p / d for p, d < 2^32: m = ceil(2^64 / d), and the error of
@@ -451,7 +437,7 @@ __global__ void __launch_bounds__(kK1Threads, 2) bucket_coarse_kernel(Src src, u
         src.ckey(static_cast<uint32_t>(p), c);
         b = upper_bound_u64(ss, ns, code_of<KW>(c, 0, P.dense));
       }
-      const unsigned rk = warp_aggregated_add(hist, static_cast<unsigned>(b), valid);
+      const unsigned rk = valid ? atomicAdd(&hist[b], 1u) : 0u;
       br[r] = (static_cast<uint32_t>(b) << 16) | rk;
     }
     __syncthreads();
@@ -821,7 +807,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
         f = upper_bound_u64(fs, ns, code_of<KW>(c, Lp, densep));
         P.fid_tmp[base + t] = static_cast<uint16_t>(f);
       }
-      warp_aggregated_add(cnt, static_cast<unsigned>(f), valid);
+      if (valid) atomicAdd(&cnt[f], 1u);
     }
     __syncthreads();
     if (P.trace && threadIdx.x == 0) s_tp[3] = clock64();
@@ -851,7 +837,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       const uint32_t t = t0 + threadIdx.x;
       const bool valid = t < n;
       const int f = valid ? P.fid_tmp[base + t] : 0;
-      const unsigned pos = warp_aggregated_add(cnt, static_cast<unsigned>(f), valid);
+      const unsigned pos = valid ? atomicAdd(&cnt[f], 1u) : 0u;
       if (valid) {
         const uint32_t p = P.idx_in[base + t];
         uint64_t c[KW];
