@@ -193,8 +193,42 @@ __device__ __forceinline__ bool bucket_range(const uint64_t* split, int ns, int 
   return lo <= hi;
 }
 
+// Number of sorted splitters a[0..n) whose top 12 bits are below h, for every
+// h in 0 .. 4096: the splitters sharing a code's top 12 bits are
+// a[tbl[h] .. tbl[h+1]).  Built by the block.
+constexpr int kTopBits = 12;
+__device__ __forceinline__ void build_top_table(const uint64_t* a, int n, uint16_t* tbl) {
+  for (int h = threadIdx.x; h <= (1 << kTopBits); h += blockDim.x) {
+    const uint64_t v = static_cast<uint64_t>(h) << (64 - kTopBits);
+    int lo = 0, hi = n;
+    if (h == (1 << kTopBits)) {
+      lo = n;
+    } else {
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+      }
+    }
+    tbl[h] = static_cast<uint16_t>(lo);
+  }
+}
+
 __device__ __forceinline__ int upper_bound_u64(const uint64_t* a, int n, uint64_t v) {
   int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (v < a[mid]) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// upper_bound_u64 through the top-12-bit table: only the splitters that share
+// v's top bits are searched.
+__device__ __forceinline__ int upper_bound_top(const uint64_t* a, const uint16_t* tbl, uint64_t v) {
+  const int h = static_cast<int>(v >> (64 - kTopBits));
+  int lo = tbl[h], hi = tbl[h + 1];
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     if (v < a[mid]) hi = mid;
@@ -413,9 +447,12 @@ __global__ void __launch_bounds__(kK1Threads, 2) bucket_coarse_kernel(Src src, u
   __shared__ uint64_t ss[kCoarseMax - 1];
   __shared__ unsigned hist[kCoarseMax];
   __shared__ unsigned base[kCoarseMax];
+  __shared__ uint16_t top[(1 << kTopBits) + 1];
   const int ns = P.B1 - 1;
   for (int i = threadIdx.x; i < ns; i += blockDim.x) ss[i] = P.split[i];
   for (int i = threadIdx.x; i < P.B1; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  build_top_table(ss, ns, top);
   __syncthreads();
   double mx = 0.0;
   const uint64_t tile = static_cast<uint64_t>(blockDim.x) * kK1Items;
@@ -435,7 +472,7 @@ __global__ void __launch_bounds__(kK1Threads, 2) bucket_coarse_kernel(Src src, u
         }
         uint64_t c[KW];
         src.ckey(static_cast<uint32_t>(p), c);
-        b = upper_bound_u64(ss, ns, code_of<KW>(c, 0, P.dense));
+        b = upper_bound_top(ss, top, code_of<KW>(c, 0, P.dense));
       }
       const unsigned rk = valid ? atomicAdd(&hist[b], 1u) : 0u;
       br[r] = (static_cast<uint32_t>(b) << 16) | rk;
@@ -637,7 +674,7 @@ constexpr int kPickChunk = kSample2 / kK2Threads;  // sorted samples per thread 
 static_assert(kPickChunk * kK2Threads == kSample2 && kPickChunk <= 31, "splitter pick chunks");
 
 constexpr size_t kK2Smem = sizeof(uint64_t) * (kSample2 + kFineSlots) + sizeof(int) * kFineSlots +
-                           sizeof(unsigned) * kFineSlots;
+                           sizeof(unsigned) * kFineSlots + sizeof(uint16_t) * ((1 << kTopBits) + 8);
 
 // Ascending bitonic sort of n (a power of two) words in shared memory.
 __device__ void smem_bitonic_u64(uint64_t* a, int n) {
@@ -665,6 +702,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
   uint64_t* fs = samp + kSample2;
   int* fL = reinterpret_cast<int*>(fs + kFineSlots);
   unsigned* cnt = reinterpret_cast<unsigned*>(fL + kFineSlots);
+  uint16_t* ftop = reinterpret_cast<uint16_t*>(cnt + kFineSlots);  // top-bit table of the fine splitters
   __shared__ unsigned s_job;
   __shared__ int s_ns;
   __shared__ unsigned warp_tmp[33];
@@ -795,6 +833,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       fL[f] = L | (dense_at(total, L) ? 0x10000 : 0);
       cnt[f] = 0;
     }
+    build_top_table(fs, ns, ftop);
     __syncthreads();
     // pass 1: fine bucket of every item
     for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
@@ -804,7 +843,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       if (valid) {
         uint64_t c[KW];
         src.ckey(P.idx_in[base + t], c);
-        f = upper_bound_u64(fs, ns, code_of<KW>(c, Lp, densep));
+        f = upper_bound_top(fs, ftop, code_of<KW>(c, Lp, densep));
         P.fid_tmp[base + t] = static_cast<uint16_t>(f);
       }
       if (valid) atomicAdd(&cnt[f], 1u);
