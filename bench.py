@@ -4,8 +4,9 @@ Default workload (N=1): config 2 of the reference's benchmark set --
 A (32,768 terms) x B (16,384 terms) on 100 qubits, k-local weight {2,3,4},
 then simplify (atol=1e-12): 536,870,912 products.  Metric: products simplified
 per second ("terms/s").  Other workloads: --workload commutation (config 3,
-bit-packed 262,144^2 matrix), expectation (config 4, forward + gradient),
-batched (config 5), plain (config 1 sequence).
+bit-packed 262,144^2 matrix), grouping (config 3, group_commuting qwc or
+full), expectation (config 4, forward + gradient), batched (config 5).
+Config 1 (the CPU-runnable sequence) is a parity case of the tests.
 
 * value      device-resident throughput; each step is timed with CUDA events on
              the stream the library launches on, L2 flushed between steps;

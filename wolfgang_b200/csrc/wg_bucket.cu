@@ -77,7 +77,7 @@ constexpr int kK1Items = 16;
 constexpr int kK2Threads = 512;
 constexpr int kK3Threads = 256;
 constexpr int kK3PerSM = 4;                     // final-kernel CTAs resident per SM
-constexpr int kIPT = 8;                         // items per thread in the final sort
+constexpr int kIPT = 8;                         // most records per thread in the final sort network
 constexpr int kCap = kK3Threads * kIPT;         // 2048 items per fine bucket
 constexpr int kPadded = kCap + kCap / 16;       // one spare slot per 16 (bank spread)
 constexpr int kWords = kCap / 32;
