@@ -164,7 +164,8 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
  *   WG_SORT_LSD     multi-word LSD radix sort of full keys;
  *   WG_SORT_BUCKET  bucketed sort on 64-bit key codes (1-2 mask words, at most
  *                   255 significant key bits); falls back to WG_SORT_LSD when a
- *                   bucket exceeds its capacity.
+ *                   bucket of mixed keys exceeds its capacity or one tie of key
+ *                   codes spans more than 16 distinct keys.
  * The setting is process-wide.  wg_last_sort_algorithm returns the algorithm
  * that produced the calling thread's last result (0 before any). */
 #define WG_SORT_AUTO 0
