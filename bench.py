@@ -108,7 +108,11 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- distributed
 
-def dist_setup(gpus: int):
+def dist_setup(gpus: int, backend: str | None = None):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE / MASTER_*).
+
+    The group only carries the barriers and the max-over-ranks timing: NCCL on
+    GPU boxes, gloo where no GPU is visible (the CPU tests of this path)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -118,8 +122,11 @@ def dist_setup(gpus: int):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -136,9 +143,16 @@ def max_over_ranks(value: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    on_gpu = dist.get_backend() == "nccl"
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if on_gpu else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard(items: list, rank: int, world: int) -> list:
+    """This rank's share of independent work units (round robin): the path has
+    no exchange step, so ranks split units and never communicate data."""
+    return items[rank::world]
 
 
 # ---------------------------------------------------------------- helpers
@@ -486,7 +500,7 @@ def bench_batched(args, world, rank, torch) -> dict:
 
     pairs = config5_pairs(args.pairs)
     if world > 1:
-        pairs = pairs[rank::world]
+        pairs = shard(pairs, rank, world)
     plans, psis = [], []
     dtype = torch.complex64 if args.c64 else torch.complex128
     for n, T, seed in pairs:
