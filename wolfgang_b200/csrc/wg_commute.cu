@@ -132,6 +132,7 @@ __global__ void fill_ones_kernel(uint32_t* bits, size_t rows, size_t cols, size_
 // is ~weight(l) shared-memory reads instead of 32 * (4W LOP3 + POPC), so for
 // sparse terms the kernel is bound by the output write.
 constexpr int kPlaneWords = 64;  // output words per row per CTA (2048 columns), two per lane
+constexpr int kRowList = 16;     // plane offsets listed per row; rows with more set bits loop over their masks
 
 template <int W>
 __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
@@ -181,9 +182,14 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
   const uint2* pl2 = reinterpret_cast<const uint2*>(planes);
   const size_t row0 = static_cast<size_t>(blockIdx.y) * rows_per_cta;
   const size_t row1 = min(n_l, row0 + rows_per_cta);
-  // A warp takes 32 rows at a time: lane r loads row rbase + r (coalesced),
-  // then each row's masks are broadcast by shuffles.  Set X bits of the row
-  // select rhs Z planes and set Z bits select rhs X planes.
+  // A warp takes 32 rows at a time: lane r loads row rbase + r (coalesced)
+  // and lists the plane offsets its row selects (set X bits select rhs Z
+  // planes, set Z bits rhs X planes); each row's list is then read by the
+  // whole warp (a broadcast), so a lane's work per set bit is one 8-byte
+  // shared-memory load and two XORs.  A row with more than kRowList set bits
+  // has its masks broadcast by shuffles and walked bit by bit instead.
+  __shared__ uint16_t lists[kWarps][32][kRowList];
+  __shared__ uint8_t counts[kWarps][32];
   for (size_t rbase = row0 + 32 * static_cast<size_t>(warp); rbase < row1; rbase += 32 * kWarps) {
     const size_t my = rbase + lane;
     uint64_t mx[W], mz[W];
@@ -192,25 +198,52 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
       mx[w] = my < row1 ? __ldg(lx + my * W + w) : 0;
       mz[w] = my < row1 ? __ldg(lz + my * W + w) : 0;
     }
+    {
+      int cnt = 0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        for (uint64_t m = mx[w]; m; m &= m - 1) {
+          if (cnt < kRowList)
+            lists[warp][lane][cnt] = static_cast<uint16_t>(((w * 64 + __ffsll(m) - 1) * 2 + 1) * (kPlaneWords / 2));
+          ++cnt;
+        }
+        for (uint64_t m = mz[w]; m; m &= m - 1) {
+          if (cnt < kRowList)
+            lists[warp][lane][cnt] = static_cast<uint16_t>(((w * 64 + __ffsll(m) - 1) * 2) * (kPlaneWords / 2));
+          ++cnt;
+        }
+      }
+      counts[warp][lane] = static_cast<uint8_t>(cnt <= kRowList ? cnt : 255);
+    }
+    __syncwarp();
     const int nrows = row1 - rbase < 32 ? static_cast<int>(row1 - rbase) : 32;
     for (int rr = 0; rr < nrows; ++rr) {
       uint2 acc = make_uint2(0u, 0u);
+      const int cnt = counts[warp][rr];
+      if (cnt != 255) {
+        for (int k = 0; k < cnt; ++k) {
+          const uint2 v = pl2[lists[warp][rr][k] + lane];
+          acc.x ^= v.x;
+          acc.y ^= v.y;
+        }
+      } else {
 #pragma unroll
-      for (int w = 0; w < W; ++w) {
-        const uint64_t ax = __shfl_sync(0xffffffffu, mx[w], rr);
-        const uint64_t az = __shfl_sync(0xffffffffu, mz[w], rr);
+        for (int w = 0; w < W; ++w) {
+          const uint64_t ax = __shfl_sync(0xffffffffu, mx[w], rr);
+          const uint64_t az = __shfl_sync(0xffffffffu, mz[w], rr);
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          const int qb = w * 64 + half * 32;
-          for (uint32_t m = static_cast<uint32_t>(ax >> (32 * half)); m; m &= m - 1) {
-            const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 1) * (kPlaneWords / 2) + lane];
-            acc.x ^= v.x;
-            acc.y ^= v.y;
-          }
-          for (uint32_t m = static_cast<uint32_t>(az >> (32 * half)); m; m &= m - 1) {
-            const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 0) * (kPlaneWords / 2) + lane];
-            acc.x ^= v.x;
-            acc.y ^= v.y;
+          for (int half = 0; half < 2; ++half) {
+            const int qb = w * 64 + half * 32;
+            for (uint32_t m = static_cast<uint32_t>(ax >> (32 * half)); m; m &= m - 1) {
+              const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 1) * (kPlaneWords / 2) + lane];
+              acc.x ^= v.x;
+              acc.y ^= v.y;
+            }
+            for (uint32_t m = static_cast<uint32_t>(az >> (32 * half)); m; m &= m - 1) {
+              const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 0) * (kPlaneWords / 2) + lane];
+              acc.x ^= v.x;
+              acc.y ^= v.y;
+            }
           }
         }
       }
@@ -222,6 +255,7 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
         if (write_ok[1]) bits[rowoff + wi[1]] = ~acc.y & valid[1];
       }
     }
+    __syncwarp();  // every lane is done with this batch's lists
   }
 }
 
