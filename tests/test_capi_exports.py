@@ -50,3 +50,33 @@ def test_invalid_arguments_are_rejected_before_device_work():
     rc = L.wg_simplify(0, 1, 0, None, None, None, 0.0, 0.0, ctypes.byref(ox), ctypes.byref(oz),
                        ctypes.byref(oc), ctypes.byref(u), None)
     assert rc == capi.WG_OK and u.value == 0 and ox.value is None
+
+
+def _built_libraries():
+    from wolfgang_b200 import build
+
+    return [capi.LIB_PATH, capi.LIB_PATH.parent / "libwolfgang.so", build.module_path()]
+
+
+def test_libraries_share_the_system_libstdcxx():
+    """Every shared library links libstdc++ dynamically and exports no unique
+    (u) symbols: a static copy would export the old std::string's empty
+    representation, and libraries loaded after it would bind to it."""
+    for path in _built_libraries():
+        needed = subprocess.run(["readelf", "-d", str(path)], capture_output=True, text=True, check=True).stdout
+        assert "libstdc++.so.6" in needed, path
+        syms = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True, text=True,
+                              check=True).stdout
+        unique = [line.split()[-1] for line in syms.splitlines() if line.split()[1:2] == ["u"]]
+        assert not unique, (path, unique[:5])
+
+
+def test_torch_imports_after_the_package():
+    """Importing the package (and its native libraries) before torch leaves
+    torch's own library loading intact."""
+    import sys
+
+    code = "import wolfgang_quantum, wolfgang_b200.capi as c; c.lib(); import torch; print('ok')"
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                         cwd=str(capi.LIB_PATH.parents[2]))
+    assert out.returncode == 0 and out.stdout.strip().endswith("ok"), (out.returncode, out.stderr[-2000:])

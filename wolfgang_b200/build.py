@@ -43,6 +43,15 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall",
              "-I", str(INCLUDE), "-I", str(HOST)]
 
+# Shared libraries link libstdc++ as the shared system library, named
+# explicitly: a toolchain whose libstdc++.so link is dangling falls back to
+# libstdc++.a, and the copy it links in exports unique symbols (the old
+# std::string's empty representation among them) that libraries loaded later
+# in the same process bind to, so that they free memory of the wrong copy
+# (torch's import crashed after this package's).  --exclude-libs hides
+# anything still taken from a static archive.
+SHARED_LINK = ["-l:libstdc++.so.6", "-Wl,--exclude-libs,ALL"]
+
 CU_SOURCES = ["wg_runtime.cu", "wg_commute.cu", "wg_simplify.cu", "wg_bucket.cu", "wg_expect.cu", "wg_group.cu"]
 CU_HEADERS = ["wg_common.cuh", "wg_scan.cuh"]
 HOST_SOURCES = ["pauli_sum.cpp", "device.cpp"]
@@ -110,7 +119,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     host_objs = [OBJ / ("host_" + Path(s).stem + ".o") for s in HOST_SOURCES]
     if _stale(wolfgang, host_objs + [wgpauli]):
         _run([CXX, "-shared", "-o", str(wolfgang), *map(str, host_objs), f"-L{LIB}", "-lwgpauli",
-              "-Wl,-rpath,$ORIGIN"])
+              "-Wl,-rpath,$ORIGIN", *SHARED_LINK])
 
     # 3. Python module
     import pybind11
@@ -120,7 +129,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     if _stale(mod, [msrc, wolfgang] + host_deps):
         _run([CXX, *CXX_FLAGS, "-shared", "-o", str(mod), str(msrc),
               "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
-              f"-L{LIB}", "-lwolfgang", "-lwgpauli", "-Wl,-rpath,$ORIGIN/lib"])
+              f"-L{LIB}", "-lwolfgang", "-lwgpauli", "-Wl,-rpath,$ORIGIN/lib", *SHARED_LINK])
     if verbose:
         print(f"built {wgpauli}, {wolfgang}, {mod}")
     return mod
