@@ -302,9 +302,9 @@ def bench_products(args, world, rank, torch) -> dict:
                    "survey_bytes_per_step": 2 * P * 48 + U * 48,
                    "survey_effective_GBps": (2 * P * 48 + U * 48) / (ms_per_step * 1e-3) / 1e9},
         # DRAM bytes per item of bucket_final_kernel measured by ncu (read + write,
-        # 1017.1 MB for a 33,554,432-product case of this workload)
+        # 1015.0 MB for a 33,554,432-product case of this workload)
         "roofline": roofline(prof, per_launch, peak, peak_kind,
-                             traffic={"bucket_final_kernel": int(P * 1017.1e6 / 33554432)}),
+                             traffic={"bucket_final_kernel": int(P * 1015.0e6 / 33554432)}),
         "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
         "gpu_launches": launches,
         "clocks": clocks.summary(),

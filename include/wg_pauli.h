@@ -164,8 +164,9 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
  *   WG_SORT_LSD     multi-word LSD radix sort of full keys;
  *   WG_SORT_BUCKET  bucketed sort on 64-bit key codes (1-2 mask words, at most
  *                   255 significant key bits); falls back to WG_SORT_LSD when a
- *                   bucket of mixed keys exceeds its capacity or one tie of key
- *                   codes spans more than 16 distinct keys.
+ *                   bucket of mixed keys stays over its capacity after being
+ *                   split again, or one tie of key codes spans more than 16
+ *                   distinct keys.
  * The setting is process-wide.  wg_last_sort_algorithm returns the algorithm
  * that produced the calling thread's last result (0 before any). */
 #define WG_SORT_AUTO 0
@@ -173,6 +174,13 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
 #define WG_SORT_BUCKET 2
 int wg_set_sort_algorithm(int algo);
 int wg_last_sort_algorithm(void);
+
+/* Target items per fine bucket of WG_SORT_BUCKET (process-wide; 0 restores
+ * the default, 896).  No reference counterpart; a tuning setting that changes
+ * no result bit.  Fine buckets that come out over their capacity of 2048 items
+ * are split again from their own samples before the final sort; a larger
+ * target means fewer, fuller buckets.  Accepts 0 or 32..2048. */
+int wg_set_bucket_fine_target(unsigned items);
 
 /* -------------------------------------------------------- expectation ---- */
 /* <psi|H|psi> (PauliSum::expectation_statevector_complex{128,64},

@@ -146,6 +146,38 @@ def test_bucket_tie_heavy_position_codes(cuda, oracle, algo):
     assert same(got, oracle.simplify(120, *raw, 1e-12, 0.0))
 
 
+@pytest.mark.parametrize("target", [1800, 1200])
+def test_bucket_fine_buckets_split_again(cuda, oracle, algo, monkeypatch, capfd, target):
+    """A fine-bucket target near the 2048-item capacity puts about one fine
+    bucket in eight over it; each is split again from its own samples, so the
+    bucketed path finishes without falling back and gives the oracle's bits.
+    At 1200 items no bucket needs it."""
+    import re
+
+    rng = seeded("bucket-refine", target)
+    _, x, z, c = random_operator(rng, 40, 400_000, 0.25, 150_000)
+    algo(capi.WG_SORT_BUCKET)
+    monkeypatch.setenv("WG_BUCKET_TRACE", "1")
+    capi.set_bucket_fine_target(target)
+    try:
+        got = G.simplify(40, x, z, c)
+        algo_used = capi.last_sort_algorithm()
+    finally:
+        capi.set_bucket_fine_target(0)
+    err = capfd.readouterr().err
+    refined = [int(v) for v in re.findall(r"refined=(\d+)", err)]
+    assert algo_used == capi.WG_SORT_BUCKET
+    assert refined and (refined[-1] > 0) == (target == 1800)
+    assert same(got, oracle.simplify(40, x, z, c))
+
+
+def test_bucket_fine_target_rejects_out_of_range(cuda):
+    for bad in (1, 31, 2049):
+        with pytest.raises(capi.WGInvalid):
+            capi.set_bucket_fine_target(bad)
+    capi.set_bucket_fine_target(0)
+
+
 @pytest.mark.parametrize("copies,bucketed", [(1500, True), (3500, True), (5000, True)])
 def test_bucket_one_key_runs(cuda, oracle, algo, copies, bucketed):
     """One key of 14 set bits repeated: its eight-digit code does not fix the

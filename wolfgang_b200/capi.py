@@ -68,6 +68,7 @@ _SIGNATURES: dict[str, list] = {
     "wg_pauli_products": [_i, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _sz, _i, _d, _d, _pvp, _pvp, _pvp, _psz, _vp],
     "wg_set_sort_algorithm": [_i],
     "wg_last_sort_algorithm": [],
+    "wg_set_bucket_fine_target": [ctypes.c_uint],
     "wg_expect_plan_create": [_i, _sz, _sz, _vp, _vp, _vp, _pvp, _vp],
     "wg_expect_plan_destroy": [_vp],
     "wg_expect_plan_set_coeffs": [_vp, _vp, _vp],
@@ -161,6 +162,11 @@ def last_sort_algorithm() -> int:
 
 
 _sort_setting = [WG_SORT_AUTO]
+
+
+def set_bucket_fine_target(items: int) -> None:
+    """Target items per fine bucket of the bucketed sort (0: the default, 896); results do not change."""
+    check(lib().wg_set_bucket_fine_target(int(items)))
 
 
 def kernel_launches() -> int:

@@ -67,10 +67,12 @@ using wgd::c128;
 constexpr int kCoarseLog = 18;           // about 2^18 items per coarse bucket
 constexpr int kCoarseMax = 2048;         // coarse buckets
 constexpr int kCoarseSample = 128;       // samples per coarse bucket
-constexpr int kFineAvg = 640;            // target items per fine bucket
-constexpr int kFineMax = 896;            // target fine buckets per coarse bucket
-constexpr int kFineSlots = 1152;         // fine bucket slots per coarse bucket (targets + isolated codes)
-constexpr int kSample2 = 8192;           // in-bucket sample for fine splitters (about 20 per fine bucket)
+constexpr int kFineAvg = 896;            // target items per fine bucket (default; settable at run time)
+constexpr int kFineMax = 640;            // target fine buckets per coarse bucket
+constexpr int kFineSlots = 832;          // fine bucket slots per coarse bucket (targets + isolated codes)
+constexpr int kSample2 = 8192;           // in-bucket sample for fine splitters (about 28 per fine bucket)
+constexpr int kRefineRounds = 4;         // rounds of extra splitters for fine buckets over capacity
+constexpr int kRefineMax = 32;           // fine buckets split in one round
 constexpr int kHeavyRun = 3;             // sample repeats that may isolate a code
 constexpr int kK1Threads = 512;
 constexpr int kK1Items = 16;
@@ -103,6 +105,7 @@ struct Control {
   unsigned fine_total;
   unsigned max_fine;             // largest fine bucket
   unsigned long long tie_items;  // items in runs of equal 8-digit codes (traced runs)
+  unsigned refined;              // fine buckets split again after counting
   unsigned long long phase[4];   // final-kernel cycles per phase (traced runs)
   unsigned long long fphase[5];  // fine-kernel cycles per phase (traced runs)
 };
@@ -220,6 +223,17 @@ __device__ __forceinline__ int upper_bound_u64(const uint64_t* a, int n, uint64_
     const int mid = (lo + hi) >> 1;
     if (v < a[mid]) hi = mid;
     else lo = mid + 1;
+  }
+  return lo;
+}
+
+// First position in the sorted a[0..n) whose value is not below v.
+__device__ __forceinline__ int lower_bound_u64(const uint64_t* a, int n, uint64_t v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < v) lo = mid + 1;
+    else hi = mid;
   }
   return lo;
 }
@@ -507,15 +521,15 @@ __global__ void __launch_bounds__(kK1Threads, 2) bucket_coarse_kernel(Src src, u
 
 // ------------------------------------------------------------------ plan
 
-__device__ __forceinline__ unsigned fine_target(unsigned n) {
-  const unsigned f = (n + kFineAvg - 1) / kFineAvg;
+__device__ __forceinline__ unsigned fine_target(unsigned n, unsigned favg) {
+  const unsigned f = (n + favg - 1) / favg;
   return f < 1 ? 1u : (f > kFineMax ? static_cast<unsigned>(kFineMax) : f);
 }
 
 // Fine bucket slots of a coarse bucket: the target count, a quarter more for
 // codes isolated on their own, and a few spare.
-__device__ __forceinline__ unsigned fine_slots(unsigned n) {
-  const unsigned t = fine_target(n);
+__device__ __forceinline__ unsigned fine_slots(unsigned n, unsigned favg) {
+  const unsigned t = fine_target(n, favg);
   return t + t / 4 + 8;
 }
 
@@ -554,7 +568,7 @@ __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* w
 __global__ void __launch_bounds__(1024) bucket_plan_kernel(const unsigned* __restrict__ fill, int B1, uint32_t capc,
                                                            const uint64_t* __restrict__ split, int total, bool dense0,
                                                            int thr_mode, double atol, double rtol, double thr_fixed,
-                                                           Control* ctl, uint32_t* __restrict__ fine_base,
+                                                           unsigned favg, Control* ctl, uint32_t* __restrict__ fine_base,
                                                            int* __restrict__ Lj) {
   __shared__ unsigned warp_tmp[33];
   unsigned carry = 0;
@@ -564,7 +578,7 @@ __global__ void __launch_bounds__(1024) bucket_plan_kernel(const unsigned* __res
     if (j < B1) {
       const unsigned c = fill[j];
       if (c > capc) atomicOr(&ctl->flags, kFlagCoarseFull);
-      slots = fine_slots(min(c, capc));
+      slots = fine_slots(min(c, capc), favg);
       uint64_t lo, hi;
       const int L = bucket_range(split, B1 - 1, j, lo, hi) ? child_prefix(0, dense0, total, lo, hi) : total;
       Lj[j] = L | (dense_at(total, L) ? 0x10000 : 0);
@@ -606,6 +620,7 @@ struct FineParams {
   uint32_t* fine_count;       // [G] count | kExactBit | kPureBit
   uint16_t* fine_L;           // [G] prefix of the bucket's codes
   Control* ctl;
+  unsigned favg;              // target items per fine bucket
   int trace;                  // record per-phase cycles
 };
 
@@ -673,6 +688,33 @@ __device__ int block_suffix_min_excl(int v, int* tmp) {
 constexpr int kPickChunk = kSample2 / kK2Threads;  // sorted samples per thread in the splitter pick
 static_assert(kPickChunk * kK2Threads == kSample2 && kPickChunk <= 31, "splitter pick chunks");
 
+// Prefix (and dense flag) of every fine bucket's codes under ns splitters;
+// slots past the last bucket take the full length.
+__device__ __forceinline__ void fine_prefixes(const uint64_t* fs, int ns, int slots, int Lp, bool densep, int total,
+                                              int* fL) {
+  for (int f = threadIdx.x; f < slots; f += blockDim.x) {
+    uint64_t lo, hi;
+    const int L = f <= ns && bucket_range(fs, ns, f, lo, hi) ? child_prefix(Lp, densep, total, lo, hi) : total;
+    fL[f] = L | (dense_at(total, L) ? 0x10000 : 0);
+  }
+}
+
+// A splitter v with lo < v <= hi for the fine bucket of codes [lo, hi] (lo <
+// hi): the median of the bucket's samples; the next sampled code above lo when
+// that median is lo itself, or lo + 1 when there is none; the middle of the
+// range when no sample falls in it.
+__device__ uint64_t refine_splitter(const uint64_t* samp, int S2, uint64_t lo, uint64_t hi) {
+  const int a = lower_bound_u64(samp, S2, lo);
+  const int b = upper_bound_u64(samp, S2, hi);
+  if (a >= b) return lo + (hi - lo) / 2 + 1;
+  const uint64_t m = samp[a + (b - a) / 2];
+  if (m > lo) return m;
+  const int c = a + upper_bound_u64(samp + a, b - a, lo);
+  return c < b ? samp[c] : lo + 1;
+}
+
+constexpr int kSplitBit = 0x40000000;  // fL flag during refinement: the bucket was split
+
 constexpr size_t kK2Smem = sizeof(uint64_t) * (kSample2 + kFineSlots) + sizeof(int) * kFineSlots +
                            sizeof(unsigned) * kFineSlots + sizeof(uint16_t) * ((1 << kTopBits) + 8);
 
@@ -708,6 +750,9 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
   __shared__ unsigned warp_tmp[33];
   __shared__ int s_scan[32];
   __shared__ long long s_tp[6];
+  __shared__ unsigned s_nfix;
+  __shared__ int s_fixf[kRefineMax];
+  __shared__ uint64_t s_fixv[kRefineMax];
   const int total = P.total;
   while (true) {
     if (P.trace && threadIdx.x == 0) s_tp[0] = clock64();
@@ -721,7 +766,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     const size_t rbase = static_cast<size_t>(j) * P.rstride;
     const uint32_t g0 = P.fine_base[j];
     const int slots = static_cast<int>(P.fine_base[j + 1] - g0);
-    const int target = static_cast<int>(fine_target(n));
+    const int target = static_cast<int>(fine_target(n, P.favg));
     const int Lp = P.Lj[j] & 0xffff;
     const bool densep = (P.Lj[j] >> 16) & 1;
     // random sample of codes relative to the coarse prefix, sorted
@@ -826,14 +871,9 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       }
     }
     __syncthreads();
-    const int ns = s_ns;
-    for (int f = threadIdx.x; f < slots; f += blockDim.x) {
-      uint64_t lo, hi;
-      const int L = f <= ns && bucket_range(fs, ns, f, lo, hi) ? child_prefix(Lp, densep, total, lo, hi) : total;
-      fL[f] = L | (dense_at(total, L) ? 0x10000 : 0);
-      cnt[f] = 0;
-    }
-    build_top_table(fs, ns, ftop);
+    fine_prefixes(fs, s_ns, slots, Lp, densep, total, fL);
+    for (int f = threadIdx.x; f < slots; f += blockDim.x) cnt[f] = 0;
+    build_top_table(fs, s_ns, ftop);
     __syncthreads();
     // pass 1: fine bucket of every item
     for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
@@ -849,6 +889,82 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       if (valid) atomicAdd(&cnt[f], 1u);
     }
     __syncthreads();
+    // Refinement.  The sample puts about 2.5 times the mean into the largest of
+    // a million fine buckets; one over kCap items whose range holds more than
+    // one code gets one more splitter from its own samples (refine_splitter),
+    // up to kRefineMax buckets a round.  Only the split buckets' items are
+    // searched again; every other item's bucket id moves up by the number of
+    // splitters inserted below it.  A bucket still over capacity after
+    // kRefineRounds rounds, or with no room left for a splitter, is flagged by
+    // the final kernel, as before.
+    for (int round = 0; round < kRefineRounds; ++round) {
+      const int ns = s_ns;
+      if (threadIdx.x == 0) s_nfix = 0;
+      __syncthreads();
+      for (int f = threadIdx.x; f <= ns; f += blockDim.x) {
+        uint64_t lo, hi;
+        if (cnt[f] > static_cast<unsigned>(kCap) && bucket_range(fs, ns, f, lo, hi) && lo < hi) {
+          const unsigned q = atomicAdd(&s_nfix, 1u);
+          if (q < static_cast<unsigned>(kRefineMax)) s_fixf[q] = f;
+        }
+      }
+      __syncthreads();
+      if (s_nfix == 0) break;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        // the split buckets in ascending order, as many as there are free slots
+        const int m = min(min(static_cast<int>(s_nfix), kRefineMax), slots - 1 - ns);
+        for (int q = 1; q < m; ++q) {
+          const int v = s_fixf[q];
+          int r = q;
+          for (; r > 0 && s_fixf[r - 1] > v; --r) s_fixf[r] = s_fixf[r - 1];
+          s_fixf[r] = v;
+        }
+        for (int q = 0; q < m; ++q) {
+          uint64_t lo, hi;
+          bucket_range(fs, ns, s_fixf[q], lo, hi);
+          s_fixv[q] = refine_splitter(samp, S2, lo, hi);
+        }
+        // splitters rewritten in place from the back: bucket b's new splitter
+        // goes just before old splitter b; fL[b] takes the shift of bucket b's
+        // id and whether it was split
+        if (m > 0) {
+          int w = ns + m - 1, q = m - 1;
+          for (int b = ns; b >= 0; --b) {
+            if (b < ns) fs[w--] = fs[b];
+            const bool sp = q >= 0 && s_fixf[q] == b;
+            if (sp) fs[w--] = s_fixv[q--];
+            fL[b] = (q + 1) | (sp ? kSplitBit : 0);
+          }
+          s_ns = ns + m;
+          atomicAdd(&P.ctl->refined, static_cast<unsigned>(m));
+        }
+        s_nfix = static_cast<unsigned>(m);
+      }
+      __syncthreads();
+      if (s_nfix == 0) break;
+      build_top_table(fs, s_ns, ftop);
+      for (int f = threadIdx.x; f < slots; f += blockDim.x) cnt[f] = 0;
+      __syncthreads();
+      for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        if (t < n) {
+          const int f = P.fid_tmp[base + t];
+          const int sh = fL[f];
+          int nf = f + (sh & ~kSplitBit);
+          if (sh & kSplitBit) {
+            uint64_t c[KW];
+            src.ckey(P.idx_in[base + t], c);
+            nf = upper_bound_top(fs, ftop, code_of<KW>(c, Lp, densep));
+          }
+          if (nf != f) P.fid_tmp[base + t] = static_cast<uint16_t>(nf);
+          atomicAdd(&cnt[nf], 1u);
+        }
+      }
+      __syncthreads();
+      fine_prefixes(fs, s_ns, slots, Lp, densep, total, fL);
+      __syncthreads();
+    }
     if (P.trace && threadIdx.x == 0) s_tp[3] = clock64();
     // fine bucket offsets, each bucket starting on a multiple of 32 records
     // (slots <= kFineSlots: a few rounds of the block scan)
@@ -1498,6 +1614,7 @@ __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParam
 // ------------------------------------------------------------------ host side
 
 std::atomic<int> g_sort_algorithm{WG_SORT_AUTO};
+std::atomic<unsigned> g_fine_target{0};  // target items per fine bucket; 0: kFineAvg
 thread_local int t_last_sort = 0;
 
 struct ThrSpec {
@@ -1555,11 +1672,13 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   while (B1 < kCoarseMax && (static_cast<uint64_t>(B1) << kCoarseLog) < n) B1 <<= 1;
   const uint64_t avg = (static_cast<uint64_t>(n) + B1 - 1) / B1;
   const uint64_t capc64 = 2 * avg + 8192;
-  if (capc64 > static_cast<uint64_t>(kFineMax) * kFineAvg) return false;  // fine buckets would overflow
+  const unsigned set_avg = g_fine_target.load(std::memory_order_relaxed);
+  const unsigned favg = set_avg ? set_avg : static_cast<unsigned>(kFineAvg);
+  if (capc64 > static_cast<uint64_t>(kFineMax) * favg) return false;  // fine buckets would overflow
   const uint32_t capc = static_cast<uint32_t>(capc64);
   const size_t region = static_cast<size_t>(B1) * capc;
-  // fine slots: sum over coarse buckets of t + t/4 + 8 with t <= n_j/kFineAvg + 1
-  const size_t Gmax = (static_cast<size_t>(n) / kFineAvg + B1) * 5 / 4 + static_cast<size_t>(B1) * 9 + 1;
+  // fine slots: sum over coarse buckets of t + t/4 + 8 with t <= n_j/favg + 1
+  const size_t Gmax = (static_cast<size_t>(n) / favg + B1) * 5 / 4 + static_cast<size_t>(B1) * 9 + 1;
   // records of the fine partition: rstride slots per coarse bucket, every fine
   // bucket starting on a multiple of 32
   const uint64_t rstride64 = ((static_cast<uint64_t>(capc) + 31) & ~uint64_t{31}) + 32ull * kFineSlots;
@@ -1611,7 +1730,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   int* Lj = ws.take_as<int>(B1);
   WG_TIMED("bucket_plan_kernel", s,
     bucket_plan_kernel<<<1, 1024, 0, s>>>(fill, B1, capc, split, total, dense0, thr.mode, thr.atol, thr.rtol,
-                                          thr.fixed, dctl, fine_base, Lj));
+                                          thr.fixed, favg, dctl, fine_base, Lj));
   wg::check_launch("launch bucket plan");
   stamp("coarse");
 
@@ -1624,7 +1743,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   {
     uint16_t* fid_tmp = ws.take_as<uint16_t>(region);
     const FineParams fp{fill, capc, B1, total, fine_base, Lj, idx1, fid_tmp, rstride, rec_code, rec_idx,
-                        fine_start, fine_count, fine_L, dctl, trace ? 1 : 0};
+                        fine_start, fine_count, fine_L, dctl, favg, trace ? 1 : 0};
     auto* k2 = bucket_fine_kernel<KW, Src>;
     set_smem(k2, kK2Smem);
     int per_sm = 0;
@@ -1664,8 +1783,9 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   wg::check_cuda(cudaStreamSynchronize(s), "synchronize bucket sort");
   stamp("sync");
   if (trace) {
-    std::fprintf(stderr, "bucket: n=%u coarse=%d fine=%u max_fine=%u flags=0x%x survivors=%u tie_items=%llu\n", n, B1,
-                 h.fine_total, h.max_fine, h.flags, U32, h.tie_items);
+    std::fprintf(stderr,
+                 "bucket: n=%u coarse=%d fine=%u max_fine=%u refined=%u flags=0x%x survivors=%u tie_items=%llu\n", n,
+                 B1, h.fine_total, h.max_fine, h.refined, h.flags, U32, h.tie_items);
     std::fprintf(stderr, "bucket final phases (Gcycles, all CTAs): load %.2f sort %.2f ties %.2f sums %.2f\n",
                  h.phase[0] * 1e-9, h.phase[1] * 1e-9, h.phase[2] * 1e-9, h.phase[3] * 1e-9);
     std::fprintf(stderr,
@@ -1804,5 +1924,13 @@ int wg_set_sort_algorithm(int algo) {
 }
 
 int wg_last_sort_algorithm(void) { return t_last_sort; }
+
+int wg_set_bucket_fine_target(unsigned items) {
+  return wg::guarded([&] {
+    if (items != 0 && (items < 32 || items > static_cast<unsigned>(kCap)))
+      wg::throw_invalid("fine bucket target must be 0 (default) or between 32 and 2048 items");
+    g_fine_target.store(items, std::memory_order_relaxed);
+  });
+}
 
 }  // extern "C"
