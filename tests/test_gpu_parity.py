@@ -286,7 +286,13 @@ def test_z_counts_match_oracle(cuda, oracle):
 
 @pytest.mark.parametrize("mode", ["qwc", "full"])
 @pytest.mark.parametrize("n,T,p,pool", [(4, 30, 0.5, None), (10, 300, 0.2, None), (70, 400, 0.05, 250),
-                                        (128, 3000, 0.05, None), (0, 5, 0.0, None)])
+                                        (128, 3000, 0.05, None), (0, 5, 0.0, None),
+                                        # many chunks of 1,024 terms; 3 and 4 mask words; repeated keys
+                                        (128, 12000, 0.05, None), (64, 9000, 0.1, 3000),
+                                        (200, 5000, 0.03, None), (256, 2500, 0.02, None),
+                                        # dense terms: about one qwc group per term, more groups than
+                                        # shared memory holds (the bases stay in global memory)
+                                        (128, 8000, 0.5, None)])
 def test_group_commuting_matches_oracle(cuda, oracle, mode, n, T, p, pool):
     import ctypes
 

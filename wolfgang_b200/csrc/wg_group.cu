@@ -7,12 +7,15 @@
 //   full: a term joins the first group all of whose members commute with it
 //                                                                  (:96-126)
 //   otherwise it opens a new group.  Groups list members in placement order.
-// The greedy is inherently sequential over terms; per term, one CTA of 1024
-// threads examines all existing groups in parallel and takes the smallest
-// accepting group index, so the result equals the sequential first-fit.
+// The first-fit is sequential over terms; here it runs in chunks: a bound pass
+// over the whole GPU finds, for every term of a chunk, the first group that
+// accepts it at the chunk's start, and one warp then places the chunk's terms
+// in order starting from those bounds (see group_bound_kernel), so the result
+// equals the sequential first-fit.
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <vector>
 
@@ -22,7 +25,6 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kGreedyThreads = 1024;
 
 // Sort keys for the deterministic order: word 0 = (maxw - weight) so that an
 // ascending sort puts heavier terms first, then the canonical key words.
@@ -55,76 +57,258 @@ __global__ void gather_terms_kernel(const uint64_t* __restrict__ x, const uint64
   }
 }
 
-// Sequential first-fit over ordered terms (ox/oz in processing order).
-// qwc state: bx/bz [G][W] group bases.  full state: first[g] / next[pos]
-// singly linked member lists (positions in processing order).
+// First-fit over ordered terms (ox/oz in processing order), in chunks of
+// kChunk terms.  Group state only grows (a qwc basis gains bits, a full-mode
+// group gains members), so a term's set of accepting groups only shrinks as
+// terms are placed: the first group that accepts a term at the start of its
+// chunk is a lower bound on the group it joins.  group_bound_kernel finds
+// that bound for every term of a chunk at once (a warp per term, 32 groups per
+// ballot); group_resolve_kernel then places the chunk's terms one by one from
+// their bounds, checking groups from the bound upward against the current
+// state, which is the sequential first-fit's answer.  In full mode the bound
+// group itself was checked against every member present at the chunk's start,
+// so only the members it gained during the chunk are checked again.
+// qwc state: one basis row per group, rows[g] = [x words | z words] (2W
+// words, moved as 16-byte pieces).  full state: first[g] / last[g] /
+// next[pos] member lists in processing order, and per group the first member
+// placed during the current chunk (cfirst[g], valid when ctag[g] is the chunk).
+constexpr int kChunk = 1024;      // terms per chunk (qwc); also the staging capacity
+constexpr int kChunkFull = 256;   // terms per chunk in full mode
+constexpr int kBoundThreads = 256;
+constexpr int kResolveThreads = 256;
+
+template <int W>
+__device__ __forceinline__ void load_row(const uint64_t* p, uint64_t (&r)[2 * W]) {
+  const ulonglong2* q = reinterpret_cast<const ulonglong2*>(p);
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    const ulonglong2 v = q[j];
+    r[2 * j] = v.x;
+    r[2 * j + 1] = v.y;
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void store_row(uint64_t* p, const uint64_t (&r)[2 * W]) {
+  ulonglong2* q = reinterpret_cast<ulonglong2*>(p);
+#pragma unroll
+  for (int j = 0; j < W; ++j) q[j] = make_ulonglong2(r[2 * j], r[2 * j + 1]);
+}
+
+// qwc: no qubit on which the term and the basis hold different non-identity
+// Paulis.  Rows are [x words | z words].
+template <int W>
+__device__ __forceinline__ bool row_accepts(const uint64_t (&t)[2 * W], const uint64_t (&b)[2 * W]) {
+  uint64_t d = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) d |= (t[w] & b[W + w]) ^ (t[W + w] & b[w]);
+  return d == 0;
+}
+
+// Every member from position m on (following next) commutes with the term.
+template <int W>
+__device__ __forceinline__ bool members_commute(const uint64_t (&t)[2 * W], const uint64_t* __restrict__ ox,
+                                                const uint64_t* __restrict__ oz, const uint32_t* next, uint32_t m) {
+  for (; m != UINT_MAX; m = next[m]) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+      acc ^= (t[w] & oz[static_cast<size_t>(m) * W + w]) ^ (t[W + w] & ox[static_cast<size_t>(m) * W + w]);
+    if (__popcll(acc) & 1u) return false;
+  }
+  return true;
+}
+
 template <int W, bool FULL>
-__global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const uint64_t* __restrict__ ox,
-                                                               const uint64_t* __restrict__ oz, uint32_t T,
-                                                               uint64_t* __restrict__ bx, uint64_t* __restrict__ bz,
-                                                               uint32_t* __restrict__ first, uint32_t* __restrict__ last,
-                                                               uint32_t* __restrict__ next, uint32_t* __restrict__ group_of,
-                                                               uint32_t* __restrict__ n_groups) {
-  __shared__ unsigned s_best;
-  uint32_t G = 0;
-  for (uint32_t i = 0; i < T; ++i) {
-    uint64_t tx[W], tz[W];
+__global__ void __launch_bounds__(kBoundThreads) group_bound_kernel(const uint64_t* __restrict__ ox,
+                                                                   const uint64_t* __restrict__ oz, uint32_t c0,
+                                                                   uint32_t c1, const uint64_t* __restrict__ rows,
+                                                                   const uint32_t* __restrict__ first,
+                                                                   const uint32_t* __restrict__ next,
+                                                                   const uint32_t* __restrict__ n_groups,
+                                                                   uint32_t* __restrict__ lb) {
+  const uint32_t G0 = *n_groups;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < c1; i += nw) {
+    uint64_t t[2 * W];
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      tx[w] = ox[static_cast<size_t>(i) * W + w];
-      tz[w] = oz[static_cast<size_t>(i) * W + w];
+      t[w] = ox[static_cast<size_t>(i) * W + w];
+      t[W + w] = oz[static_cast<size_t>(i) * W + w];
     }
-    if (threadIdx.x == 0) s_best = UINT_MAX;
-    __syncthreads();
-    for (uint32_t g = threadIdx.x; g < G; g += kGreedyThreads) {
-      if (g >= *static_cast<volatile unsigned*>(&s_best)) break;
-      bool accept = true;
-      if (!FULL) {
-#pragma unroll
-        for (int w = 0; w < W; ++w)
-          accept = accept && (((tx[w] & bz[static_cast<size_t>(g) * W + w]) ^ (tz[w] & bx[static_cast<size_t>(g) * W + w])) == 0);
-      } else {
-        for (uint32_t m = first[g]; m != UINT_MAX; m = next[m]) {
-          uint64_t acc = 0;
-#pragma unroll
-          for (int w = 0; w < W; ++w)
-            acc ^= (tx[w] & oz[static_cast<size_t>(m) * W + w]) ^ (tz[w] & ox[static_cast<size_t>(m) * W + w]);
-          if (__popcll(acc) & 1u) {
-            accept = false;
-            break;
-          }
+    uint32_t found = G0;
+    for (uint32_t g0 = 0; g0 < G0; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      bool ok = false;
+      if (g < G0) {
+        if (FULL) {
+          ok = members_commute<W>(t, ox, oz, next, first[g]);
+        } else {
+          uint64_t r[2 * W];
+          load_row<W>(rows + static_cast<size_t>(g) * (2 * W), r);
+          ok = row_accepts<W>(t, r);
         }
       }
-      if (accept) {
-        atomicMin(&s_best, g);
+      const unsigned b = __ballot_sync(0xffffffffu, ok);
+      if (b) {
+        found = g0 + __ffs(b) - 1;
         break;
       }
     }
-    __syncthreads();
-    uint32_t best = s_best;
+    if (lane == 0) lb[i] = found;
+  }
+}
+
+// qwc placement of a chunk's staged term rows by one warp.  Lane j owns the
+// groups g with g % 32 == j: any 32 consecutive groups hold one group of each
+// lane, so a round over [g0, g0 + 32) has lane j check g0 + ((j - g0) & 31),
+// and a basis row is only ever read and written by its owner (no cross-lane
+// ordering is needed).  One warp reduction per round gives the smallest
+// accepting group; its owner ORs the term into the row.  The fast loop runs
+// the first round of each term (most terms end there) and leaves at the first
+// term it cannot place; that term's later rounds (or its new group) are
+// handled outside it, and the fast loop resumes.  Keeping the rare path out of
+// the per-term loop keeps the loop free of nested warp-synchronous control
+// flow.  B holds the basis rows: shared memory (SMEM) or global memory.
+template <int W, bool SMEM>
+__device__ __forceinline__ uint32_t place_qwc(const uint64_t* st, const uint32_t* slb, uint32_t* sgid, uint32_t n,
+                                              uint32_t G, uint64_t* B) {
+  const uint32_t lane = threadIdx.x & 31;
+  auto row_at = [&](uint32_t g) { return SMEM ? B + g * (2 * W) : B + static_cast<size_t>(g) * (2 * W); };
+  uint32_t k = 0;
+  while (k < n) {
+    uint64_t t[2 * W], r[2 * W];
+    uint32_t l = 0;
+    for (; k < n; ++k) {
+      load_row<W>(st + k * (2 * W), t);
+      l = slb[k];
+      const uint32_t g = l + ((lane - l) & 31u);
+      bool ok = false;
+      if (g < G) {
+        load_row<W>(row_at(g), r);
+        ok = row_accepts<W>(t, r);
+      }
+      const uint32_t best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+      if (best == UINT_MAX) break;
+      if (best % 32 == lane) {
+#pragma unroll
+        for (int e = 0; e < 2 * W; ++e) r[e] |= t[e];
+        store_row<W>(row_at(best), r);
+      }
+      if (lane == 0) sgid[k] = best;
+    }
+    if (k >= n) break;
+    // term k: the rounds after the first, then a new group if none accepts
+    uint32_t best = UINT_MAX;
+    for (uint32_t g0 = l + 32; best == UINT_MAX && g0 < G; g0 += 32) {
+      const uint32_t g = g0 + ((lane - g0) & 31u);
+      bool ok = false;
+      if (g < G) {
+        load_row<W>(row_at(g), r);
+        ok = row_accepts<W>(t, r);
+      }
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
     const bool fresh = best == UINT_MAX;
     if (fresh) best = G;
-    if (threadIdx.x == 0) {
-      group_of[i] = best;
-      if (!FULL) {
+    if (best % 32 == lane) {
 #pragma unroll
-        for (int w = 0; w < W; ++w) {
-          const size_t o = static_cast<size_t>(best) * W + w;
-          bx[o] = fresh ? tx[w] : (bx[o] | tx[w]);
-          bz[o] = fresh ? tz[w] : (bz[o] | tz[w]);
-        }
-      } else {
-        next[i] = UINT_MAX;
-        if (fresh) first[best] = i;
-        else next[last[best]] = i;
-        last[best] = i;
-      }
-      __threadfence_block();
+      for (int e = 0; e < 2 * W; ++e) r[e] = fresh ? t[e] : (r[e] | t[e]);
+      store_row<W>(row_at(best), r);
     }
     if (fresh) ++G;
-    __syncthreads();
+    if (lane == 0) sgid[k] = best;
+    ++k;
   }
-  if (threadIdx.x == 0) *n_groups = G;
+  return G;
+}
+
+// One CTA: its threads stage the chunk's term rows and bounds (and, in qwc
+// mode, the basis rows when every group of the chunk fits) in shared memory;
+// warp 0 places the terms in order; the threads then write the basis rows
+// back and the chunk's group ids out.
+template <int W, bool FULL>
+__global__ void __launch_bounds__(kResolveThreads) group_resolve_kernel(
+    const uint64_t* __restrict__ ox, const uint64_t* __restrict__ oz, uint32_t c0, uint32_t c1, uint32_t tag,
+    uint32_t cap, uint64_t* __restrict__ rows, uint32_t* __restrict__ first, uint32_t* __restrict__ last,
+    uint32_t* __restrict__ next, uint32_t* __restrict__ cfirst, uint32_t* __restrict__ ctag,
+    const uint32_t* __restrict__ lb, uint32_t* __restrict__ group_of, uint32_t* __restrict__ n_groups) {
+  extern __shared__ __align__(16) unsigned char rraw[];
+  __shared__ uint32_t s_G;
+  const uint32_t n = c1 - c0;
+  uint64_t* st = reinterpret_cast<uint64_t*>(rraw);         // [kChunk][2W] term rows
+  uint64_t* sb = st + kChunk * (2 * W);                       // [cap][2W] basis rows
+  uint32_t* slb = reinterpret_cast<uint32_t*>(sb + static_cast<size_t>(cap) * (2 * W));
+  uint32_t* sgid = slb + kChunk;
+  const uint32_t G0 = *n_groups;
+  const bool in_smem = !FULL && static_cast<uint64_t>(G0) + n <= cap;
+  for (uint32_t k = threadIdx.x; k < n * W; k += blockDim.x) {
+    const uint32_t kk = k / W, w = k - kk * W;
+    st[kk * (2 * W) + w] = ox[static_cast<size_t>(c0) * W + k];
+    st[kk * (2 * W) + W + w] = oz[static_cast<size_t>(c0) * W + k];
+  }
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) slb[k] = lb[c0 + k];
+  if (in_smem) {
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(rows);
+    ulonglong2* dst = reinterpret_cast<ulonglong2*>(sb);
+    for (uint32_t k = threadIdx.x; k < G0 * W; k += blockDim.x) dst[k] = src[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t G = G0;
+    if (!FULL) {
+      G = in_smem ? place_qwc<W, true>(st, slb, sgid, n, G0, sb) : place_qwc<W, false>(st, slb, sgid, n, G0, rows);
+    } else {
+      const int lane = threadIdx.x;
+      for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t i = c0 + k;
+        uint64_t t[2 * W];
+        load_row<W>(st + k * (2 * W), t);
+        const uint32_t l = slb[k];
+        uint32_t best = G;
+        for (uint32_t g0 = l; g0 < G; g0 += 32) {
+          const uint32_t g = g0 + lane;
+          bool ok = false;
+          if (g < G) {
+            // the bound group was checked against its members at the chunk's start
+            const uint32_t m = g == l && g < G0 ? (ctag[g] == tag ? cfirst[g] : UINT_MAX) : first[g];
+            ok = members_commute<W>(t, ox, oz, next, m);
+          }
+          const uint32_t m_ok = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+          if (m_ok != UINT_MAX) {
+            best = m_ok;
+            break;
+          }
+        }
+        const bool fresh = best == G;
+        if (lane == 0) {
+          sgid[k] = best;
+          next[i] = UINT_MAX;
+          if (fresh) first[best] = i;
+          else next[last[best]] = i;
+          last[best] = i;
+          if (ctag[best] != tag) {
+            ctag[best] = tag;
+            cfirst[best] = i;
+          }
+        }
+        if (fresh) ++G;
+        __syncwarp();
+      }
+    }
+    if (threadIdx.x == 0) {
+      *n_groups = G;
+      s_G = G;
+    }
+  }
+  __syncthreads();
+  if (in_smem) {
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(sb);
+    ulonglong2* dst = reinterpret_cast<ulonglong2*>(rows);
+    for (uint32_t k = threadIdx.x; k < s_G * W; k += blockDim.x) dst[k] = src[k];
+  }
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) group_of[c0 + k] = sgid[k];
 }
 
 // 64-bit sort keys from group ids; carried index = processing position.
@@ -154,15 +338,38 @@ __global__ void group_out_kernel(const uint32_t* __restrict__ order, const uint3
 }
 
 template <int W>
-void launch_greedy(bool full, const uint64_t* ox, const uint64_t* oz, uint32_t T, uint64_t* bx, uint64_t* bz,
-                   uint32_t* first, uint32_t* last, uint32_t* next, uint32_t* gid, uint32_t* ng, cudaStream_t s) {
-  if (full)
-    WG_TIMED("greedy_kernel", s,
-      greedy_kernel<W, true><<<1, kGreedyThreads, 0, s>>>(ox, oz, T, bx, bz, first, last, next, gid, ng));
-  else
-    WG_TIMED("greedy_kernel", s,
-      greedy_kernel<W, false><<<1, kGreedyThreads, 0, s>>>(ox, oz, T, bx, bz, first, last, next, gid, ng));
-  wg::check_launch("launch group greedy");
+void run_greedy(int device, bool full, const uint64_t* ox, const uint64_t* oz, uint32_t T, uint64_t* rows,
+                uint32_t* first, uint32_t* last, uint32_t* next, uint32_t* cfirst, uint32_t* ctag, uint32_t* lb,
+                uint32_t* gid, uint32_t* ng, cudaStream_t s) {
+  const auto& props = wg::device_props(device);
+  auto* kb = full ? group_bound_kernel<W, true> : group_bound_kernel<W, false>;
+  auto* kr = full ? group_resolve_kernel<W, true> : group_resolve_kernel<W, false>;
+  // term rows, bounds and group ids of a chunk, then as many basis rows as fit
+  // beside the kernel's static shared memory
+  cudaFuncAttributes fa{};
+  wg::check_cuda(cudaFuncGetAttributes(&fa, kr), "query group resolve attributes");
+  const size_t stage = static_cast<size_t>(kChunk) * (16 * W + 8);
+  const size_t smem_max = static_cast<size_t>(props.max_smem_optin) - fa.sharedSizeBytes;
+  const uint32_t cap = full || smem_max <= stage ? 0u : static_cast<uint32_t>((smem_max - stage) / (16 * W));
+  const size_t smem = stage + static_cast<size_t>(cap) * 16 * W;
+  wg::check_cuda(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                 "set group resolve shared memory");
+  wg::check_cuda(cudaMemsetAsync(ng, 0, 4, s), "clear group count");
+  if (full) wg::check_cuda(cudaMemsetAsync(ctag, 0xff, 4 * static_cast<size_t>(T), s), "clear chunk tags");
+  const unsigned max_blocks = static_cast<unsigned>(props.sm_count) * 8;
+  // full mode re-walks member lists on every failed candidate: shorter chunks
+  // keep the bounds closer to the answers
+  const uint32_t chunk = full ? kChunkFull : kChunk;
+  uint32_t tag = 0;
+  for (uint32_t c0 = 0; c0 < T; c0 += chunk, ++tag) {
+    const uint32_t c1 = T - c0 > chunk ? c0 + chunk : T;
+    const unsigned blocks = std::min<unsigned>(max_blocks, (c1 - c0 + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
+    WG_TIMED("group_bound_kernel", s, kb<<<blocks, kBoundThreads, 0, s>>>(ox, oz, c0, c1, rows, first, next, ng, lb));
+    wg::check_launch("launch group bounds");
+    WG_TIMED("group_resolve_kernel", s,
+      kr<<<1, kResolveThreads, smem, s>>>(ox, oz, c0, c1, tag, cap, rows, first, last, next, cfirst, ctag, lb, gid, ng));
+    wg::check_launch("launch group resolve");
+  }
 }
 
 // ---------------------------------------------------------------- Z counts
@@ -252,23 +459,27 @@ int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t*
       wg::check_cuda(cudaMemsetAsync(ox.get(), 0, 8 * T, s), "clear masks");
       wg::check_cuda(cudaMemsetAsync(oz.get(), 0, 8 * T, s), "clear masks");
     }
-    wg::Scratch bx(8 * Wa * T, s), bz(8 * Wa * T, s), first(4 * T, s), last(4 * T, s), next(4 * T, s),
-        gid(4 * T, s), ng(4, s);
+    wg::Scratch rows(16 * Wa * T, s), first(4 * T, s), last(4 * T, s), next(4 * T, s),
+        cfirst(4 * T, s), ctag(4 * T, s), lb(4 * T, s), gid(4 * T, s), ng(4, s);
     const bool full = mode_full != 0;
     const uint32_t T32 = static_cast<uint32_t>(T);
     switch (W) {
       case 0:
-      case 1: launch_greedy<1>(full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, bx.as<uint64_t>(), bz.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), gid.as<uint32_t>(),
+      case 1: run_greedy<1>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
+                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
-      case 2: launch_greedy<2>(full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, bx.as<uint64_t>(), bz.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), gid.as<uint32_t>(),
+      case 2: run_greedy<2>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
+                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
-      case 3: launch_greedy<3>(full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, bx.as<uint64_t>(), bz.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), gid.as<uint32_t>(),
+      case 3: run_greedy<3>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
+                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
-      default: launch_greedy<4>(full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, bx.as<uint64_t>(), bz.as<uint64_t>(),
-                                first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), gid.as<uint32_t>(),
+      default: run_greedy<4>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
+                                first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
+                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
                                 ng.as<uint32_t>(), s); break;
     }
     uint32_t G = 0;
