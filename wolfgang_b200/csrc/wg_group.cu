@@ -70,8 +70,9 @@ __global__ void gather_terms_kernel(const uint64_t* __restrict__ x, const uint64
 // so only the members it gained during the chunk are checked again.
 // qwc state: one basis row per group, rows[g] = [x words | z words] (2W
 // words, moved as 16-byte pieces).  full state: first[g] / last[g] /
-// next[pos] member lists in processing order, and per group the first member
-// placed during the current chunk (cfirst[g], valid when ctag[g] is the chunk).
+// next[pos] member lists in processing order; the bound pass also records
+// which of the 32 groups from the bound accepted the term at the chunk's start
+// (lbm), so that those need checking only against the chunk's own members.
 constexpr int kChunk = 1024;      // terms per chunk (qwc); also the staging capacity
 constexpr int kChunkFull = 256;   // terms per chunk in full mode
 constexpr int kBoundThreads = 256;
@@ -119,6 +120,17 @@ __device__ __forceinline__ bool members_commute(const uint64_t (&t)[2 * W], cons
   return true;
 }
 
+// The term anticommutes with the staged row (2W words in shared memory).
+template <int W>
+__device__ __forceinline__ bool anticommutes(const uint64_t (&t)[2 * W], const uint64_t* row) {
+  uint64_t r[2 * W];
+  load_row<W>(row, r);
+  uint64_t acc = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) acc ^= (t[w] & r[W + w]) ^ (t[W + w] & r[w]);
+  return (__popcll(acc) & 1u) != 0;
+}
+
 template <int W, bool FULL>
 __global__ void __launch_bounds__(kBoundThreads) group_bound_kernel(const uint64_t* __restrict__ ox,
                                                                    const uint64_t* __restrict__ oz, uint32_t c0,
@@ -126,7 +138,8 @@ __global__ void __launch_bounds__(kBoundThreads) group_bound_kernel(const uint64
                                                                    const uint32_t* __restrict__ first,
                                                                    const uint32_t* __restrict__ next,
                                                                    const uint32_t* __restrict__ n_groups,
-                                                                   uint32_t* __restrict__ lb) {
+                                                                   uint32_t* __restrict__ lb,
+                                                                   uint32_t* __restrict__ lbm) {
   const uint32_t G0 = *n_groups;
   const int lane = threadIdx.x & 31;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -157,6 +170,13 @@ __global__ void __launch_bounds__(kBoundThreads) group_bound_kernel(const uint64
       }
     }
     if (lane == 0) lb[i] = found;
+    if (FULL) {
+      // which of the 32 groups from the bound accept the term now
+      const uint32_t g = found + lane;
+      const bool ok = g < G0 && members_commute<W>(t, ox, oz, next, first[g]);
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (lane == 0) lbm[i] = m;
+    }
   }
 }
 
@@ -224,16 +244,92 @@ __device__ __forceinline__ uint32_t place_qwc(const uint64_t* st, const uint32_t
   return G;
 }
 
+// Full-mode placement of a chunk's staged term rows by one warp.  A term's
+// bound group l accepted it at the chunk's start, so the fast loop checks it
+// only against the chunk's members placed in l so far (lane-parallel over the
+// chunk's earlier terms, one vote).  A term that fails, or had no bound, goes
+// through the groups in first-fit order outside the fast loop: the window
+// groups that accepted it at the chunk's start (lbm), again against the
+// chunk's members only; the older groups beyond the window, by a walk of their
+// whole member list; the groups opened during the chunk, whose members are all
+// chunk members.  sgid[k] is written by lane k % 32, the lane that reads it in
+// the fast loop; the slow path starts with a warp barrier so that every lane
+// sees all group ids and list links written so far.
+template <int W>
+__device__ __forceinline__ uint32_t place_full(const uint64_t* __restrict__ ox, const uint64_t* __restrict__ oz,
+                                               const uint64_t* st, const uint32_t* slb, const uint32_t* smask,
+                                               uint32_t* sgid, uint32_t n, uint32_t c0, uint32_t G0, uint32_t* first,
+                                               uint32_t* last, uint32_t* next) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t G = G0;
+  // no member placed in group g among the chunk's first k terms anticommutes with t
+  auto chunk_members_commute = [&](const uint64_t (&t)[2 * W], uint32_t g, uint32_t k) {
+    for (uint32_t q = 0; q < k; ++q)
+      if (sgid[q] == g && anticommutes<W>(t, st + q * (2 * W))) return false;
+    return true;
+  };
+  auto place = [&](uint32_t k, uint32_t best, bool fresh) {
+    if ((k & 31u) == lane) sgid[k] = best;
+    if (lane == 0) {
+      const uint32_t i = c0 + k;
+      next[i] = UINT_MAX;
+      if (fresh) first[best] = i;
+      else next[last[best]] = i;
+      last[best] = i;
+    }
+  };
+  uint32_t k = 0;
+  while (k < n) {
+    uint64_t t[2 * W];
+    uint32_t l = 0;
+    for (; k < n; ++k) {
+      load_row<W>(st + k * (2 * W), t);
+      l = slb[k];
+      if (l >= G0) break;
+      bool bad = false;
+      for (uint32_t q = lane; q < k; q += 32)
+        if (sgid[q] == l && anticommutes<W>(t, st + q * (2 * W))) bad = true;
+      if (__any_sync(0xffffffffu, bad)) break;
+      place(k, l, false);
+    }
+    if (k >= n) break;
+    __syncwarp();
+    const uint32_t m = smask[k];
+    uint32_t best = UINT_MAX;
+    {
+      const uint32_t g = l + lane;
+      const bool ok = l < G0 && lane > 0 && g < G0 && ((m >> lane) & 1u) && chunk_members_commute(t, g, k);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    for (uint32_t g0 = l + 32; best == UINT_MAX && g0 < G0; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      const bool ok = g < G0 && members_commute<W>(t, ox, oz, next, first[g]);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    for (uint32_t g0 = G0; best == UINT_MAX && g0 < G; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      const bool ok = g < G && chunk_members_commute(t, g, k);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    const bool fresh = best == UINT_MAX;
+    if (fresh) best = G;
+    place(k, best, fresh);
+    if (fresh) ++G;
+    __syncwarp();
+    ++k;
+  }
+  return G;
+}
+
 // One CTA: its threads stage the chunk's term rows and bounds (and, in qwc
 // mode, the basis rows when every group of the chunk fits) in shared memory;
 // warp 0 places the terms in order; the threads then write the basis rows
 // back and the chunk's group ids out.
 template <int W, bool FULL>
 __global__ void __launch_bounds__(kResolveThreads) group_resolve_kernel(
-    const uint64_t* __restrict__ ox, const uint64_t* __restrict__ oz, uint32_t c0, uint32_t c1, uint32_t tag,
-    uint32_t cap, uint64_t* __restrict__ rows, uint32_t* __restrict__ first, uint32_t* __restrict__ last,
-    uint32_t* __restrict__ next, uint32_t* __restrict__ cfirst, uint32_t* __restrict__ ctag,
-    const uint32_t* __restrict__ lb, uint32_t* __restrict__ group_of, uint32_t* __restrict__ n_groups) {
+    const uint64_t* __restrict__ ox, const uint64_t* __restrict__ oz, uint32_t c0, uint32_t c1, uint32_t cap, uint64_t* __restrict__ rows, uint32_t* __restrict__ first, uint32_t* __restrict__ last,
+    uint32_t* __restrict__ next, const uint32_t* __restrict__ lb, const uint32_t* __restrict__ lbm,
+    uint32_t* __restrict__ group_of, uint32_t* __restrict__ n_groups) {
   extern __shared__ __align__(16) unsigned char rraw[];
   __shared__ uint32_t s_G;
   const uint32_t n = c1 - c0;
@@ -241,6 +337,7 @@ __global__ void __launch_bounds__(kResolveThreads) group_resolve_kernel(
   uint64_t* sb = st + kChunk * (2 * W);                       // [cap][2W] basis rows
   uint32_t* slb = reinterpret_cast<uint32_t*>(sb + static_cast<size_t>(cap) * (2 * W));
   uint32_t* sgid = slb + kChunk;
+  uint32_t* smask = sgid + kChunk;
   const uint32_t G0 = *n_groups;
   const bool in_smem = !FULL && static_cast<uint64_t>(G0) + n <= cap;
   for (uint32_t k = threadIdx.x; k < n * W; k += blockDim.x) {
@@ -248,7 +345,10 @@ __global__ void __launch_bounds__(kResolveThreads) group_resolve_kernel(
     st[kk * (2 * W) + w] = ox[static_cast<size_t>(c0) * W + k];
     st[kk * (2 * W) + W + w] = oz[static_cast<size_t>(c0) * W + k];
   }
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) slb[k] = lb[c0 + k];
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    slb[k] = lb[c0 + k];
+    if (FULL) smask[k] = lbm[c0 + k];
+  }
   if (in_smem) {
     const ulonglong2* src = reinterpret_cast<const ulonglong2*>(rows);
     ulonglong2* dst = reinterpret_cast<ulonglong2*>(sb);
@@ -260,42 +360,7 @@ __global__ void __launch_bounds__(kResolveThreads) group_resolve_kernel(
     if (!FULL) {
       G = in_smem ? place_qwc<W, true>(st, slb, sgid, n, G0, sb) : place_qwc<W, false>(st, slb, sgid, n, G0, rows);
     } else {
-      const int lane = threadIdx.x;
-      for (uint32_t k = 0; k < n; ++k) {
-        const uint32_t i = c0 + k;
-        uint64_t t[2 * W];
-        load_row<W>(st + k * (2 * W), t);
-        const uint32_t l = slb[k];
-        uint32_t best = G;
-        for (uint32_t g0 = l; g0 < G; g0 += 32) {
-          const uint32_t g = g0 + lane;
-          bool ok = false;
-          if (g < G) {
-            // the bound group was checked against its members at the chunk's start
-            const uint32_t m = g == l && g < G0 ? (ctag[g] == tag ? cfirst[g] : UINT_MAX) : first[g];
-            ok = members_commute<W>(t, ox, oz, next, m);
-          }
-          const uint32_t m_ok = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
-          if (m_ok != UINT_MAX) {
-            best = m_ok;
-            break;
-          }
-        }
-        const bool fresh = best == G;
-        if (lane == 0) {
-          sgid[k] = best;
-          next[i] = UINT_MAX;
-          if (fresh) first[best] = i;
-          else next[last[best]] = i;
-          last[best] = i;
-          if (ctag[best] != tag) {
-            ctag[best] = tag;
-            cfirst[best] = i;
-          }
-        }
-        if (fresh) ++G;
-        __syncwarp();
-      }
+      G = place_full<W>(ox, oz, st, slb, smask, sgid, n, c0, G0, first, last, next);
     }
     if (threadIdx.x == 0) {
       *n_groups = G;
@@ -339,35 +404,34 @@ __global__ void group_out_kernel(const uint32_t* __restrict__ order, const uint3
 
 template <int W>
 void run_greedy(int device, bool full, const uint64_t* ox, const uint64_t* oz, uint32_t T, uint64_t* rows,
-                uint32_t* first, uint32_t* last, uint32_t* next, uint32_t* cfirst, uint32_t* ctag, uint32_t* lb,
-                uint32_t* gid, uint32_t* ng, cudaStream_t s) {
+                uint32_t* first, uint32_t* last, uint32_t* next, uint32_t* lb, uint32_t* lbm, uint32_t* gid,
+                uint32_t* ng, cudaStream_t s) {
   const auto& props = wg::device_props(device);
   auto* kb = full ? group_bound_kernel<W, true> : group_bound_kernel<W, false>;
   auto* kr = full ? group_resolve_kernel<W, true> : group_resolve_kernel<W, false>;
-  // term rows, bounds and group ids of a chunk, then as many basis rows as fit
+  // term rows, bounds, bound masks and group ids of a chunk, then as many basis rows as fit
   // beside the kernel's static shared memory
   cudaFuncAttributes fa{};
   wg::check_cuda(cudaFuncGetAttributes(&fa, kr), "query group resolve attributes");
-  const size_t stage = static_cast<size_t>(kChunk) * (16 * W + 8);
+  const size_t stage = static_cast<size_t>(kChunk) * (16 * W + 12);
   const size_t smem_max = static_cast<size_t>(props.max_smem_optin) - fa.sharedSizeBytes;
   const uint32_t cap = full || smem_max <= stage ? 0u : static_cast<uint32_t>((smem_max - stage) / (16 * W));
   const size_t smem = stage + static_cast<size_t>(cap) * 16 * W;
   wg::check_cuda(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                  "set group resolve shared memory");
   wg::check_cuda(cudaMemsetAsync(ng, 0, 4, s), "clear group count");
-  if (full) wg::check_cuda(cudaMemsetAsync(ctag, 0xff, 4 * static_cast<size_t>(T), s), "clear chunk tags");
   const unsigned max_blocks = static_cast<unsigned>(props.sm_count) * 8;
   // full mode re-walks member lists on every failed candidate: shorter chunks
   // keep the bounds closer to the answers
   const uint32_t chunk = full ? kChunkFull : kChunk;
-  uint32_t tag = 0;
-  for (uint32_t c0 = 0; c0 < T; c0 += chunk, ++tag) {
+  for (uint32_t c0 = 0; c0 < T; c0 += chunk) {
     const uint32_t c1 = T - c0 > chunk ? c0 + chunk : T;
     const unsigned blocks = std::min<unsigned>(max_blocks, (c1 - c0 + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
-    WG_TIMED("group_bound_kernel", s, kb<<<blocks, kBoundThreads, 0, s>>>(ox, oz, c0, c1, rows, first, next, ng, lb));
+    WG_TIMED("group_bound_kernel", s,
+      kb<<<blocks, kBoundThreads, 0, s>>>(ox, oz, c0, c1, rows, first, next, ng, lb, lbm));
     wg::check_launch("launch group bounds");
     WG_TIMED("group_resolve_kernel", s,
-      kr<<<1, kResolveThreads, smem, s>>>(ox, oz, c0, c1, tag, cap, rows, first, last, next, cfirst, ctag, lb, gid, ng));
+      kr<<<1, kResolveThreads, smem, s>>>(ox, oz, c0, c1, cap, rows, first, last, next, lb, lbm, gid, ng));
     wg::check_launch("launch group resolve");
   }
 }
@@ -459,27 +523,27 @@ int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t*
       wg::check_cuda(cudaMemsetAsync(ox.get(), 0, 8 * T, s), "clear masks");
       wg::check_cuda(cudaMemsetAsync(oz.get(), 0, 8 * T, s), "clear masks");
     }
-    wg::Scratch rows(16 * Wa * T, s), first(4 * T, s), last(4 * T, s), next(4 * T, s),
-        cfirst(4 * T, s), ctag(4 * T, s), lb(4 * T, s), gid(4 * T, s), ng(4, s);
+    wg::Scratch rows(16 * Wa * T, s), first(4 * T, s), last(4 * T, s), next(4 * T, s), lb(4 * T, s), lbm(4 * T, s),
+        gid(4 * T, s), ng(4, s);
     const bool full = mode_full != 0;
     const uint32_t T32 = static_cast<uint32_t>(T);
     switch (W) {
       case 0:
       case 1: run_greedy<1>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
-                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
+                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
       case 2: run_greedy<2>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
-                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
+                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
       case 3: run_greedy<3>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
-                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
+                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
       default: run_greedy<4>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                                first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), cfirst.as<uint32_t>(),
-                               ctag.as<uint32_t>(), lb.as<uint32_t>(), gid.as<uint32_t>(),
+                                first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
+                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
                                 ng.as<uint32_t>(), s); break;
     }
     uint32_t G = 0;
