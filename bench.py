@@ -327,9 +327,13 @@ def bench_products(args, world, rank, torch) -> dict:
         concurrent = max_over_ranks(0.0 if fits else 1.0, world) == 0.0
 
         def e2e_calls() -> tuple[float, int]:
-            hA.matmul(hB, max_intermediate_terms=P)  # warm
+            r = hA.matmul(hB, max_intermediate_terms=P)  # warm
             t0 = time.perf_counter()
             for _ in range(args.e2e_steps):
+                # each step is one call: the previous step's result is released
+                # first (inside the timed region), so that a call does not run
+                # beside another 24 GB result
+                r = None
                 r = hA.matmul(hB, max_intermediate_terms=P)
             dt_, terms_ = (time.perf_counter() - t0) / args.e2e_steps, r.num_terms
             del r

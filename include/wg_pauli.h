@@ -60,6 +60,15 @@ int wg_free(int device, void* ptr, wg_stream_t stream);
 int wg_memcpy_htod(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
 int wg_memcpy_dtoh(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
 int wg_memcpy_dtod(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
+/* Device-to-host copy delivered in chunks: the buffer goes through pinned
+ * staging and each chunk is handed, in order, to fn(user, chunk, chunk_bytes)
+ * on the calling thread once it has landed (chunks are 64 MiB, the last one
+ * shorter).  Lets a caller build its own host container from the data without
+ * first filling it (e.g. appending to a reserved std::vector).  Calls from
+ * different threads run concurrently, each with its own staging and stream.
+ * No reference counterpart (the reference downloads into resized vectors). */
+typedef void (*wg_chunk_fn)(void* user, const void* chunk, size_t chunk_bytes);
+int wg_memcpy_dtoh_chunked(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user);
 int wg_memset(int device, void* dst, int value, size_t bytes, wg_stream_t stream);
 int wg_stream_synchronize(int device, wg_stream_t stream);
 int wg_device_synchronize(int device);

@@ -245,18 +245,20 @@ def test_sort_algorithm_rejects_unknown(cuda):
         capi.set_sort_algorithm(7)
 
 
-def test_public_matmul_large_host_result(cuda, algo):
+@pytest.mark.parametrize("nl,nr", [(2048, 1024), (4096, 2048)])
+def test_public_matmul_large_host_result(cuda, algo, nl, nr):
     """PauliSum.matmul through the public API with a host result above 64 MiB
-    (the pre-faulted, concurrently initialised result vectors) equals the
-    device-side products of the C-ABI, downloaded directly."""
+    (pre-faulted result vectors filled by appending the downloaded chunks; the
+    larger case spans several 64 MiB chunks per vector) equals the device-side
+    products of the C-ABI, downloaded directly."""
     import wolfgang_quantum as wq
 
-    rng = seeded("public-large")
-    A = klocal(rng, 100, 2048)
-    B = klocal(rng, 100, 1024)
+    rng = seeded("public-large", nl, nr)
+    A = klocal(rng, 100, nl)
+    B = klocal(rng, 100, nr)
     hA = wq.PauliSum._from_packed(100, A[1], A[2], A[3])
     hB = wq.PauliSum._from_packed(100, B[1], B[2], B[3])
-    r = hA.matmul(hB, max_intermediate_terms=2048 * 1024)
+    r = hA.matmul(hB, max_intermediate_terms=nl * nr)
     x, z, c = r._packed()
     assert x.nbytes + z.nbytes + c.nbytes >= 64 << 20
     gx, gz, gc = G.products(100, A[1:], B[1:], capi.WG_PRODUCTS_FUSED)

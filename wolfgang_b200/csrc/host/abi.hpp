@@ -4,6 +4,7 @@
 // these functions.
 
 #include <cstddef>
+#include <vector>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -62,6 +63,18 @@ class DeviceBuffer {
   }
   void download(void* dst, std::size_t bytes) const {
     if (bytes) check(wg_memcpy_dtoh(device_, dst, ptr_, bytes, nullptr));
+  }
+  // Appends the buffer's first `count` elements to v, chunk by chunk, without
+  // first filling v: reserve v's capacity beforehand.
+  template <typename T>
+  void append_to(std::vector<T>& v, std::size_t count) const {
+    if (count == 0) return;
+    auto fn = [](void* user, const void* chunk, std::size_t bytes) {
+      auto* out = static_cast<std::vector<T>*>(user);
+      const T* b = static_cast<const T*>(chunk);
+      out->insert(out->end(), b, b + bytes / sizeof(T));
+    };
+    check(wg_memcpy_dtoh_chunked(device_, ptr_, count * sizeof(T), fn, &v));
   }
   template <typename T>
   T* as() const {

@@ -11,6 +11,7 @@
 #include <bit>
 #include <cmath>
 #include <complex>
+#include <exception>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -40,11 +41,13 @@ void set_bit(std::vector<std::uint64_t>& v, std::size_t words, std::size_t term,
 char letter(bool xb, bool zb) { return xb ? (zb ? 'Y' : 'X') : (zb ? 'Z' : 'I'); }
 
 // Result vectors of a large download.  A value-initialised std::vector of
-// many gigabytes spends most of its construction taking 4 KiB page faults one
-// at a time.  Here the storage is reserved first, advised for transparent huge
-// pages and pre-faulted by several threads (MADV_POPULATE_WRITE over disjoint
-// ranges), and the vectors are then value-initialised concurrently over
-// resident memory.  Small results take the plain path.
+// many gigabytes spends its construction on page faults and on writing zeros
+// that the download then overwrites.  Here the storage is reserved, advised
+// for transparent huge pages and pre-faulted by several threads
+// (MADV_POPULATE_WRITE over disjoint ranges); the vectors are then filled by
+// appending the downloaded chunks (each element written once), x, z and the
+// coefficients concurrently, each through its own pinned staging.  Small
+// results take the plain path.
 constexpr std::size_t kBigHostBytes = std::size_t{64} << 20;
 
 void prefault(void* p, std::size_t bytes, unsigned threads) {
@@ -66,12 +69,16 @@ void prefault(void* p, std::size_t bytes, unsigned threads) {
 #endif
 }
 
-void make_result_vectors(std::size_t words_total, std::size_t terms, std::vector<std::uint64_t>& x,
-                         std::vector<std::uint64_t>& z, std::vector<std::complex<double>>& c) {
+void fetch_result_vectors(const DeviceBuffer& bx, const DeviceBuffer& bz, const DeviceBuffer& bc,
+                          std::size_t words_total, std::size_t terms, std::vector<std::uint64_t>& x,
+                          std::vector<std::uint64_t>& z, std::vector<std::complex<double>>& c) {
   if (16 * words_total + 16 * terms < kBigHostBytes) {
     x.resize(words_total);
     z.resize(words_total);
     c.resize(terms);
+    bx.download(x.data(), x.size() * 8);
+    bz.download(z.data(), z.size() * 8);
+    bc.download(c.data(), c.size() * 16);
     return;
   }
   x.reserve(words_total);
@@ -85,11 +92,31 @@ void make_result_vectors(std::size_t words_total, std::size_t terms, std::vector
     tx.join();
     tz.join();
   }
-  std::thread tx([&] { x.resize(words_total); });
-  std::thread tz([&] { z.resize(words_total); });
-  c.resize(terms);
+  std::exception_ptr ex, ez;
+  std::thread tx([&] {
+    try {
+      bx.append_to(x, words_total);
+    } catch (...) {
+      ex = std::current_exception();
+    }
+  });
+  std::thread tz([&] {
+    try {
+      bz.append_to(z, words_total);
+    } catch (...) {
+      ez = std::current_exception();
+    }
+  });
+  std::exception_ptr ec;
+  try {
+    bc.append_to(c, terms);
+  } catch (...) {
+    ec = std::current_exception();
+  }
   tx.join();
   tz.join();
+  for (const auto& e : {ex, ez, ec})
+    if (e) std::rethrow_exception(e);
 }
 
 // Operands of one compute call, resident on the compute device.
@@ -297,10 +324,7 @@ PauliSum PauliSum::download_device_result(std::size_t n, std::size_t words, int 
   if (U == 0) return PauliSum::empty(n);
   std::vector<std::uint64_t> x, z;
   std::vector<std::complex<double>> c;
-  make_result_vectors(U * words, U, x, z, c);
-  bx.download(x.data(), x.size() * 8);
-  bz.download(z.data(), z.size() * 8);
-  bc.download(c.data(), c.size() * 16);
+  fetch_result_vectors(bx, bz, bc, U * words, U, x, z, c);
   return PauliSum(n, words, U, std::move(x), std::move(z), std::move(c));
 }
 
@@ -342,10 +366,7 @@ PauliSum PauliSum::matmul(const PauliSum& rhs, bool simplify_output, std::size_t
     DeviceBuffer bc = DeviceBuffer::adopt(dev, oc, U * 16);
     std::vector<std::uint64_t> x, z;
     std::vector<std::complex<double>> c;
-    make_result_vectors(U * words_, U, x, z, c);
-    bx.download(x.data(), x.size() * 8);
-    bz.download(z.data(), z.size() * 8);
-    bc.download(c.data(), c.size() * 16);
+    fetch_result_vectors(bx, bz, bc, U * words_, U, x, z, c);
     return PauliSum(num_qubits_, words_, U, std::move(x), std::move(z), std::move(c));
   }
   return download_device_result(num_qubits_, words_, dev, ox, oz, oc, U);

@@ -167,7 +167,80 @@ void parallel_memcpy(char* dst, const char* src, size_t bytes) {
   std::memcpy(dst, src, std::min(part, bytes));
   for (auto& t : th) t.join();
 }
+// Staging for chunked downloads: one pair of pinned buffers, two events and a
+// stream per concurrent call, kept for reuse.
+struct ChunkStage {
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  cudaStream_t stream = nullptr;
+  int device = -1;
+};
+std::mutex g_chunk_mu;
+std::vector<ChunkStage*> g_chunk_free;
+
+ChunkStage* take_chunk_stage(int device) {
+  {
+    std::lock_guard<std::mutex> lk(g_chunk_mu);
+    for (size_t i = 0; i < g_chunk_free.size(); ++i) {
+      if (g_chunk_free[i]->device == device) {
+        ChunkStage* c = g_chunk_free[i];
+        g_chunk_free.erase(g_chunk_free.begin() + static_cast<std::ptrdiff_t>(i));
+        return c;
+      }
+    }
+  }
+  auto* c = new ChunkStage;
+  c->device = device;
+  try {
+    for (int i = 0; i < 2; ++i) {
+      check_cuda(cudaHostAlloc(&c->buf[i], kStageBytes, cudaHostAllocPortable), "allocate pinned staging");
+      check_cuda(cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming), "create staging event");
+    }
+    check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "create staging stream");
+  } catch (...) {
+    for (int i = 0; i < 2; ++i) {
+      if (c->buf[i]) (void)cudaFreeHost(c->buf[i]);
+      if (c->done[i]) (void)cudaEventDestroy(c->done[i]);
+    }
+    delete c;
+    throw;
+  }
+  return c;
+}
+
+void give_chunk_stage(ChunkStage* c) {
+  std::lock_guard<std::mutex> lk(g_chunk_mu);
+  g_chunk_free.push_back(c);
+}
 }  // namespace
+
+void chunked_download(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user) {
+  ChunkStage* c = take_chunk_stage(device);
+  const char* const sp = static_cast<const char*>(src);
+  const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
+  auto len_of = [&](size_t k) { return std::min(kStageBytes, bytes - k * kStageBytes); };
+  try {
+    // DMA chunk k into buffer k%2 while the caller consumes chunk k-1
+    for (size_t k = 0; k <= chunks; ++k) {
+      if (k < chunks) {
+        check_cuda(cudaMemcpyAsync(c->buf[k & 1], sp + k * kStageBytes, len_of(k), cudaMemcpyDeviceToHost,
+                                   c->stream),
+                   "copy device buffer to staging");
+        check_cuda(cudaEventRecord(c->done[k & 1], c->stream), "record staging event");
+      }
+      if (k > 0) {
+        const size_t j = k - 1;
+        check_cuda(cudaEventSynchronize(c->done[j & 1]), "wait for staging");
+        fn(user, c->buf[j & 1], len_of(j));
+      }
+    }
+  } catch (...) {
+    (void)cudaStreamSynchronize(c->stream);
+    give_chunk_stage(c);
+    throw;
+  }
+  give_chunk_stage(c);
+}
 
 bool pinned_host(const void* p) {
   cudaPointerAttributes a{};
@@ -358,6 +431,15 @@ int wg_memcpy_dtoh(int device, void* dst, const void* src, size_t bytes, wg_stre
     }
     check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream), "copy device buffer to host");
     check_cuda(cudaStreamSynchronize(stream), "synchronize copy to host");
+  });
+}
+
+int wg_memcpy_dtoh_chunked(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user) {
+  return guarded([&] {
+    if (bytes == 0) return;
+    if (fn == nullptr) throw_invalid("chunked download needs a chunk callback");
+    DeviceGuard g(device);
+    wg::chunked_download(device, src, bytes, fn, user);
   });
 }
 
