@@ -55,6 +55,25 @@ def test_commutation_algorithms_agree_on_config1(cuda):
     assert same_bits(b1, b2)
 
 
+@pytest.mark.parametrize("n", [64, 128])
+def test_commutation_wide_tiles_match(cuda, oracle, n):
+    """Both sides above 65,536 terms with one or two mask words take the
+    bit-plane kernel's 4,096-column tiles (four output words per lane, 1,024
+    threads), with a ragged last tile: bit for bit equal to the ballot
+    algorithm everywhere, and to the oracle on a slice of rows."""
+    rng = seeded("comm-wide", n)
+    nl, nr = 65536 + 77, 65536 + 1000
+    A = random_operator(rng, n, nl, 0.05)
+    B = random_operator(rng, n, nr, 0.05)
+    b2 = G.commutation_bits(n, A[1:3], B[1:3], algo=2)
+    b1 = G.commutation_bits(n, A[1:3], B[1:3], algo=1)
+    assert same_bits(b1, b2)
+    rows = np.r_[0:200, nl - 56:nl]
+    want = oracle.commutes(n, (A[1][rows], A[2][rows]), B[1:3])
+    assert np.array_equal(G.unpack_bits(b2[rows], nr), want)
+    assert np.all(b2[:, -1] >> np.uint32(nr % 32) == 0)
+
+
 def test_commutation_config3_row_slice_matches_oracle(cuda, oracle):
     from wolfgang_b200.workloads import config3
 

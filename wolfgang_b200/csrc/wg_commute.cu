@@ -125,29 +125,51 @@ __global__ void fill_ones_kernel(uint32_t* bits, size_t rows, size_t cols, size_
 }
 
 // ---------------------------------------------------------------------------
-// algo 2: bit-plane XOR.  For a block of 32*kPlaneWords rhs columns, plane
-// (q, X|Z) is the bit-vector over the block of the rhs x/z bits on qubit q.
-// Row l's output word j is the complement of XOR over q in supp(l) of
+// algo 2: bit-plane XOR.  For a block of 32*LW*32 rhs columns, plane (q,
+// X|Z) is the bit-vector over the block of the rhs x/z bits on qubit q.  Row
+// l's output word j is the complement of XOR over q in supp(l) of
 // (lx_q ? Zplane_q[j] : 0) ^ (lz_q ? Xplane_q[j] : 0).  Per output word that
 // is ~weight(l) shared-memory reads instead of 32 * (4W LOP3 + POPC), so for
-// sparse terms the kernel is bound by the output write.
-constexpr int kPlaneWords = 64;  // output words per row per CTA (2048 columns), two per lane
-constexpr int kRowList = 16;     // plane offsets listed per row; rows with more set bits loop over their masks
+// sparse terms the kernel is bound by issue, not by POPC.  Each lane owns LW
+// consecutive output words of a row (read as one LW-word vector per plane):
+// LW = 4 with 1,024 threads for large products of 1-2 mask words (planes take
+// up to 128 KB of shared memory), LW = 2 with 256 threads otherwise.
+constexpr int kRowList = 16;  // plane offsets listed per row; rows with more set bits loop over their masks
 
-template <int W>
-__global__ void __launch_bounds__(kThreads) commute_plane_kernel(
+template <int LW>
+__device__ __forceinline__ void xor_plane(uint32_t (&acc)[LW], const uint32_t* planes, int vec) {
+  if constexpr (LW == 4) {
+    const uint4 v = reinterpret_cast<const uint4*>(planes)[vec];
+    acc[0] ^= v.x;
+    acc[1] ^= v.y;
+    acc[2] ^= v.z;
+    acc[3] ^= v.w;
+  } else {
+    static_assert(LW == 2, "two or four output words per lane");
+    const uint2 v = reinterpret_cast<const uint2*>(planes)[vec];
+    acc[0] ^= v.x;
+    acc[1] ^= v.y;
+  }
+}
+
+template <int W, int LW, int THREADS>
+__global__ void __launch_bounds__(THREADS) commute_plane_kernel(
     const uint64_t* __restrict__ lx, const uint64_t* __restrict__ lz, size_t n_l,
     const uint64_t* __restrict__ rx, const uint64_t* __restrict__ rz, size_t n_r,
     uint32_t* __restrict__ bits, size_t pitch, size_t rows_per_cta) {
-  // planes[(q*2 + 0)*32 + j] = X bits of rhs block word j on qubit q; +1 = Z bits.
-  extern __shared__ uint32_t planes[];
+  constexpr int kWordsCta = 32 * LW;  // output words per row per CTA
+  constexpr int kWarpsCta = THREADS / 32;
+  // planes[(q*2 + 0)*kWordsCta + j] = X bits of rhs block word j on qubit q; +1 = Z bits.
+  // In LW-word vectors a plane is 32 vectors long, so plane p starts at vector 32p.
+  extern __shared__ __align__(16) uint32_t planes[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const size_t col0 = static_cast<size_t>(blockIdx.x) * (32 * kPlaneWords);
+  const size_t col0 = static_cast<size_t>(blockIdx.x) * (32 * kWordsCta);
   const size_t words_needed = (n_r + 31) / 32;
-  // Build: warp handles block words j = warp, warp+8, ...; lane t loads column
-  // col0 + 32j + t once, then one ballot per (qubit, x|z) gives a plane word.
-  for (int j = warp; j < kPlaneWords; j += kWarps) {
+  // Build: warp handles block words j = warp, warp + kWarpsCta, ...; lane t
+  // loads column col0 + 32j + t once, then one ballot per (qubit, x|z) gives a
+  // plane word.
+  for (int j = warp; j < kWordsCta; j += kWarpsCta) {
     const size_t c = col0 + 32 * static_cast<size_t>(j) + lane;
     const bool ok = c < n_r;
 #pragma unroll
@@ -160,37 +182,36 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
         const uint32_t pz = __ballot_sync(0xffffffffu, (vz >> b) & 1u);
         if (lane == (b & 31)) {
           const int q = w * 64 + b;
-          planes[(q * 2 + 0) * kPlaneWords + j] = px;
-          planes[(q * 2 + 1) * kPlaneWords + j] = pz;
+          planes[(q * 2 + 0) * kWordsCta + j] = px;
+          planes[(q * 2 + 1) * kWordsCta + j] = pz;
         }
       }
     }
   }
   __syncthreads();
-  // lane covers output words 2*lane and 2*lane + 1 of the block
-  uint32_t valid[2];
-  bool write_ok[2];
-  size_t wi[2];
+  // lane covers output words LW*lane .. LW*lane + LW - 1 of the block
+  uint32_t valid[LW];
+  bool write_ok[LW];
+  size_t wi[LW];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int j = 2 * lane + h;
+  for (int h = 0; h < LW; ++h) {
+    const int j = LW * lane + h;
     const size_t c_first = col0 + 32 * static_cast<size_t>(j);
     valid[h] = c_first >= n_r ? 0u : (n_r - c_first < 32 ? (1u << (n_r - c_first)) - 1u : 0xffffffffu);
-    wi[h] = static_cast<size_t>(blockIdx.x) * kPlaneWords + j;
+    wi[h] = static_cast<size_t>(blockIdx.x) * kWordsCta + j;
     write_ok[h] = wi[h] < words_needed;
   }
-  const uint2* pl2 = reinterpret_cast<const uint2*>(planes);
   const size_t row0 = static_cast<size_t>(blockIdx.y) * rows_per_cta;
   const size_t row1 = min(n_l, row0 + rows_per_cta);
   // A warp takes 32 rows at a time: lane r loads row rbase + r (coalesced)
   // and lists the plane offsets its row selects (set X bits select rhs Z
   // planes, set Z bits rhs X planes); each row's list is then read by the
-  // whole warp (a broadcast), so a lane's work per set bit is one 8-byte
-  // shared-memory load and two XORs.  A row with more than kRowList set bits
+  // whole warp (a broadcast), so a lane's work per set bit is one LW-word
+  // shared-memory load and LW XORs.  A row with more than kRowList set bits
   // has its masks broadcast by shuffles and walked bit by bit instead.
-  __shared__ uint16_t lists[kWarps][32][kRowList];
-  __shared__ uint8_t counts[kWarps][32];
-  for (size_t rbase = row0 + 32 * static_cast<size_t>(warp); rbase < row1; rbase += 32 * kWarps) {
+  __shared__ uint16_t lists[kWarpsCta][32][kRowList];
+  __shared__ uint8_t counts[kWarpsCta][32];
+  for (size_t rbase = row0 + 32 * static_cast<size_t>(warp); rbase < row1; rbase += 32 * kWarpsCta) {
     const size_t my = rbase + lane;
     uint64_t mx[W], mz[W];
 #pragma unroll
@@ -203,13 +224,11 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
 #pragma unroll
       for (int w = 0; w < W; ++w) {
         for (uint64_t m = mx[w]; m; m &= m - 1) {
-          if (cnt < kRowList)
-            lists[warp][lane][cnt] = static_cast<uint16_t>(((w * 64 + __ffsll(m) - 1) * 2 + 1) * (kPlaneWords / 2));
+          if (cnt < kRowList) lists[warp][lane][cnt] = static_cast<uint16_t>(((w * 64 + __ffsll(m) - 1) * 2 + 1) * 32);
           ++cnt;
         }
         for (uint64_t m = mz[w]; m; m &= m - 1) {
-          if (cnt < kRowList)
-            lists[warp][lane][cnt] = static_cast<uint16_t>(((w * 64 + __ffsll(m) - 1) * 2) * (kPlaneWords / 2));
+          if (cnt < kRowList) lists[warp][lane][cnt] = static_cast<uint16_t>(((w * 64 + __ffsll(m) - 1) * 2) * 32);
           ++cnt;
         }
       }
@@ -218,14 +237,12 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
     __syncwarp();
     const int nrows = row1 - rbase < 32 ? static_cast<int>(row1 - rbase) : 32;
     for (int rr = 0; rr < nrows; ++rr) {
-      uint2 acc = make_uint2(0u, 0u);
+      uint32_t acc[LW];
+#pragma unroll
+      for (int h = 0; h < LW; ++h) acc[h] = 0u;
       const int cnt = counts[warp][rr];
       if (cnt != 255) {
-        for (int k = 0; k < cnt; ++k) {
-          const uint2 v = pl2[lists[warp][rr][k] + lane];
-          acc.x ^= v.x;
-          acc.y ^= v.y;
-        }
+        for (int k = 0; k < cnt; ++k) xor_plane<LW>(acc, planes, lists[warp][rr][k] + lane);
       } else {
 #pragma unroll
         for (int w = 0; w < W; ++w) {
@@ -234,25 +251,24 @@ __global__ void __launch_bounds__(kThreads) commute_plane_kernel(
 #pragma unroll
           for (int half = 0; half < 2; ++half) {
             const int qb = w * 64 + half * 32;
-            for (uint32_t m = static_cast<uint32_t>(ax >> (32 * half)); m; m &= m - 1) {
-              const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 1) * (kPlaneWords / 2) + lane];
-              acc.x ^= v.x;
-              acc.y ^= v.y;
-            }
-            for (uint32_t m = static_cast<uint32_t>(az >> (32 * half)); m; m &= m - 1) {
-              const uint2 v = pl2[((qb + __ffs(m) - 1) * 2 + 0) * (kPlaneWords / 2) + lane];
-              acc.x ^= v.x;
-              acc.y ^= v.y;
-            }
+            for (uint32_t m = static_cast<uint32_t>(ax >> (32 * half)); m; m &= m - 1)
+              xor_plane<LW>(acc, planes, ((qb + __ffs(m) - 1) * 2 + 1) * 32 + lane);
+            for (uint32_t m = static_cast<uint32_t>(az >> (32 * half)); m; m &= m - 1)
+              xor_plane<LW>(acc, planes, ((qb + __ffs(m) - 1) * 2 + 0) * 32 + lane);
           }
         }
       }
-      const size_t rowoff = (rbase + rr) * pitch;
-      if (write_ok[0] && write_ok[1] && (reinterpret_cast<uintptr_t>(bits + rowoff + wi[0]) & 7) == 0) {
-        *reinterpret_cast<uint2*>(bits + rowoff + wi[0]) = make_uint2(~acc.x & valid[0], ~acc.y & valid[1]);
+      uint32_t* out = bits + (rbase + rr) * pitch + wi[0];
+      if (write_ok[LW - 1] && (reinterpret_cast<uintptr_t>(out) & (4 * LW - 1)) == 0) {
+        if constexpr (LW == 4)
+          *reinterpret_cast<uint4*>(out) =
+              make_uint4(~acc[0] & valid[0], ~acc[1] & valid[1], ~acc[2] & valid[2], ~acc[3] & valid[3]);
+        else
+          *reinterpret_cast<uint2*>(out) = make_uint2(~acc[0] & valid[0], ~acc[1] & valid[1]);
       } else {
-        if (write_ok[0]) bits[rowoff + wi[0]] = ~acc.x & valid[0];
-        if (write_ok[1]) bits[rowoff + wi[1]] = ~acc.y & valid[1];
+#pragma unroll
+        for (int h = 0; h < LW; ++h)
+          if (write_ok[h]) out[h] = ~acc[h] & valid[h];
       }
     }
     __syncwarp();  // every lane is done with this batch's lists
@@ -279,20 +295,19 @@ void launch_ballot(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uin
   wg::check_launch("launch commutation (ballot)");
 }
 
-template <int W>
-void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
-                  const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, int device,
-                  cudaStream_t s) {
-  const size_t smem = static_cast<size_t>(64 * W) * 2 * kPlaneWords * sizeof(uint32_t);
+template <int W, int LW, int THREADS>
+void launch_plane_as(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx, const uint64_t* rz,
+                     size_t n_r, uint32_t* bits, size_t pitch, int device, cudaStream_t s) {
+  constexpr int kWordsCta = 32 * LW;
+  auto* kernel = commute_plane_kernel<W, LW, THREADS>;
+  const size_t smem = static_cast<size_t>(64 * W) * 2 * kWordsCta * sizeof(uint32_t);
   static bool configured[64] = {};
   if (!configured[device & 63]) {
-    wg::check_cuda(cudaFuncSetAttribute(commute_plane_kernel<W>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem)),
+    wg::check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                    "configure bit-plane commutation");
     configured[device & 63] = true;
   }
-  const size_t col_blocks = (n_r + 32 * kPlaneWords - 1) / (32 * kPlaneWords);
+  const size_t col_blocks = (n_r + 32 * kWordsCta - 1) / (32 * kWordsCta);
   // Enough row chunks to fill the machine; rows per CTA amortise plane building.
   const size_t sms = wg::device_props(device).sm_count;
   size_t rows_per_cta = 2048;
@@ -305,8 +320,26 @@ void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint
   }
   dim3 grid(static_cast<unsigned>(col_blocks), static_cast<unsigned>(row_chunks));
   WG_TIMED("commute_plane_kernel", s,
-    commute_plane_kernel<W><<<grid, kThreads, smem, s>>>(lx, lz, n_l, rx, rz, n_r, bits, pitch, rows_per_cta));
+    kernel<<<grid, THREADS, smem, s>>>(lx, lz, n_l, rx, rz, n_r, bits, pitch, rows_per_cta));
   wg::check_launch("launch commutation (bit-plane)");
+}
+
+// Four output words per lane and 1,024 threads (4,096-column tiles) for one or
+// two mask words when both sides are large: measured 5.9 against 7.2 ms on
+// 262,144^2 terms.  Smaller products keep two words per lane and 256 threads,
+// where the wider tile's plane building would not be amortised over enough
+// rows (32,768^2 terms: 433 against 253 us).
+template <int W>
+void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
+                  const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, int device,
+                  cudaStream_t s) {
+  if constexpr (W <= 2) {
+    if (n_l >= 65536 && n_r >= 65536) {
+      launch_plane_as<W, 4, 1024>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
+      return;
+    }
+  }
+  launch_plane_as<W, 2, 256>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
 }
 
 // Autotuned choice between the two algorithms.  Cost model per output word:
