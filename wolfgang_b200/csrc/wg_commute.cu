@@ -308,9 +308,12 @@ void launch_plane_as(const uint64_t* lx, const uint64_t* lz, size_t n_l, const u
     configured[device & 63] = true;
   }
   const size_t col_blocks = (n_r + 32 * kWordsCta - 1) / (32 * kWordsCta);
-  // Enough row chunks to fill the machine; rows per CTA amortise plane building.
+  // Enough row chunks to fill the machine (at least four CTAs per SM); as many
+  // rows per CTA as that allows, to amortise the plane building: on 262,144^2
+  // terms 2,048 rows per CTA took 5.93 ms, 4,096 4.57, 8,192 3.88, 16,384 3.52
+  // (32,768 rows at two CTAs per SM 3.80: the last wave runs part empty).
   const size_t sms = wg::device_props(device).sm_count;
-  size_t rows_per_cta = 2048;
+  size_t rows_per_cta = 16384;
   while (rows_per_cta > 256 && col_blocks * ((n_l + rows_per_cta - 1) / rows_per_cta) < 4 * sms)
     rows_per_cta /= 2;
   size_t row_chunks = (n_l + rows_per_cta - 1) / rows_per_cta;
