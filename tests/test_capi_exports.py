@@ -80,3 +80,22 @@ def test_torch_imports_after_the_package():
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
                          cwd=str(capi.LIB_PATH.parents[2]))
     assert out.returncode == 0 and out.stdout.strip().endswith("ok"), (out.returncode, out.stderr[-2000:])
+
+
+def test_bucket_fine_target_is_range_checked_before_device_work():
+    for bad in (1, 31, 2049):
+        try:
+            capi.set_bucket_fine_target(bad)
+        except capi.WGInvalid as e:
+            assert "fine bucket target" in str(e)
+        else:
+            raise AssertionError(f"fine target {bad} accepted")
+    capi.set_bucket_fine_target(1800)
+    capi.set_bucket_fine_target(0)
+
+
+def test_chunked_download_needs_a_callback():
+    L = capi.lib()
+    rc = L.wg_memcpy_dtoh_chunked(0, None, 64, None, None)
+    assert rc == capi.WG_ERR_INVALID and b"callback" in L.wg_last_error()
+    assert L.wg_memcpy_dtoh_chunked(0, None, 0, None, None) == capi.WG_OK
