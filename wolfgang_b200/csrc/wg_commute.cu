@@ -206,9 +206,10 @@ __global__ void __launch_bounds__(THREADS) commute_plane_kernel(
   // A warp takes 32 rows at a time: lane r loads row rbase + r (coalesced)
   // and lists the plane offsets its row selects (set X bits select rhs Z
   // planes, set Z bits rhs X planes); each row's list is then read by the
-  // whole warp (a broadcast), so a lane's work per set bit is one LW-word
-  // shared-memory load and LW XORs.  A row with more than kRowList set bits
-  // has its masks broadcast by shuffles and walked bit by bit instead.
+  // whole warp (a broadcast, two offsets per 32-bit read), so a lane's work
+  // per set bit is one LW-word shared-memory load and LW XORs.  A row with
+  // more than kRowList set bits has its masks broadcast by shuffles and walked
+  // bit by bit instead.
   __shared__ uint16_t lists[kWarpsCta][32][kRowList];
   __shared__ uint8_t counts[kWarpsCta][32];
   for (size_t rbase = row0 + 32 * static_cast<size_t>(warp); rbase < row1; rbase += 32 * kWarpsCta) {
@@ -242,7 +243,14 @@ __global__ void __launch_bounds__(THREADS) commute_plane_kernel(
       for (int h = 0; h < LW; ++h) acc[h] = 0u;
       const int cnt = counts[warp][rr];
       if (cnt != 255) {
-        for (int k = 0; k < cnt; ++k) xor_plane<LW>(acc, planes, lists[warp][rr][k] + lane);
+        const uint32_t* l2 = reinterpret_cast<const uint32_t*>(lists[warp][rr]);
+        int k = 0;
+        for (; k + 1 < cnt; k += 2) {
+          const uint32_t pr = l2[k >> 1];
+          xor_plane<LW>(acc, planes, static_cast<int>(pr & 0xffffu) + lane);
+          xor_plane<LW>(acc, planes, static_cast<int>(pr >> 16) + lane);
+        }
+        if (k < cnt) xor_plane<LW>(acc, planes, lists[warp][rr][k] + lane);
       } else {
 #pragma unroll
         for (int w = 0; w < W; ++w) {
