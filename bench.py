@@ -299,8 +299,8 @@ def bench_products(args, world, rank, torch) -> dict:
                                "matmul+simplify(atol=1e-12)",
                    "products": P, "survivors": U, "words": W,
                    "l2": "intermediates >> L2 (126 MB); 512 MiB L2 flush between steps",
-                   "survey_bytes_per_step": 2 * P * 48 + U * 48,
-                   "survey_effective_GBps": (2 * P * 48 + U * 48) / (ms_per_step * 1e-3) / 1e9},
+                   "byte_model_bytes_per_step": 2 * P * 48 + U * 48,
+                   "byte_model_GBps": (2 * P * 48 + U * 48) / (ms_per_step * 1e-3) / 1e9},
         # DRAM bytes per item of bucket_final_kernel measured by ncu (read + write,
         # 1015.0 MB for a 33,554,432-product case of this workload)
         "roofline": roofline(prof, per_launch, peak, peak_kind,
@@ -532,7 +532,7 @@ def bench_expectation(args, world, rank, torch) -> dict:
             "unit": "evals/s", "ms_per_step": t, "cpu_baseline": out_cpu,
             "config": {"workload": f"config4: {n} qubits, {len(op[3])} terms, {G} x-groups, "
                                    f"{'c64' if args.c64 else 'c128'} psi, forward{'' if args.forward_only else '+adjoint'}",
-                       "survey_bytes_per_step": G * psi_bytes + (0 if args.forward_only else 2 * psi_bytes + G * psi_bytes)},
+                       "byte_model_bytes_per_step": G * psi_bytes + (0 if args.forward_only else 2 * psi_bytes + G * psi_bytes)},
             "roofline": rl, "gpu_launches": launches, "clocks": clocks,
             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
 
