@@ -135,6 +135,49 @@ __device__ __forceinline__ bool anticommutes(const uint64_t (&t)[2 * W], const u
   return (__popcll(acc) & 1u) != 0;
 }
 
+// Full mode: the bound of each term of a chunk is searched by kBoundSplit
+// warps, warp s taking every kBoundSplit-th round of 32 groups from round s.
+// A warp records the first accepting group of its rounds with atomicMin on
+// lb[i] (set to UINT_MAX beforehand) and stops once its next round starts at
+// or above the smallest group recorded so far, so lb[i] ends as the first
+// accepting group overall.  Member lists make a round of checks long; the
+// split keeps a chunk of few terms from leaving most of the GPU idle.
+constexpr int kBoundSplit = 8;
+
+template <int W>
+__global__ void __launch_bounds__(kBoundThreads) group_search_full_kernel(
+    const uint64_t* __restrict__ ox, const uint64_t* __restrict__ oz, uint32_t c0, uint32_t c1,
+    const uint32_t* __restrict__ first, const uint32_t* __restrict__ next, const uint32_t* __restrict__ n_groups,
+    uint32_t* lb) {
+  const uint32_t G0 = *n_groups;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t units = (c1 - c0) * kBoundSplit;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < units; u += nw) {
+    const uint32_t i = c0 + u / kBoundSplit, sub = u % kBoundSplit;
+    uint64_t t[2 * W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      t[w] = ox[static_cast<size_t>(i) * W + w];
+      t[W + w] = oz[static_cast<size_t>(i) * W + w];
+    }
+    for (uint32_t g0 = sub * 32; g0 < G0; g0 += 32 * kBoundSplit) {
+      // the smallest accepting group any warp has recorded, read once per warp
+      uint32_t best = 0;
+      if (lane == 0) best = *static_cast<volatile uint32_t*>(&lb[i]);
+      best = __shfl_sync(0xffffffffu, best, 0);
+      if (g0 >= best) break;
+      const uint32_t g = g0 + lane;
+      const bool ok = g < G0 && members_commute<W>(t, ox, oz, next, first[g]);
+      const unsigned b = __ballot_sync(0xffffffffu, ok);
+      if (b) {
+        if (lane == 0) atomicMin(&lb[i], g0 + __ffs(b) - 1);
+        break;
+      }
+    }
+  }
+}
+
 template <int W, bool FULL>
 __global__ void __launch_bounds__(kBoundThreads) group_bound_kernel(const uint64_t* __restrict__ ox,
                                                                    const uint64_t* __restrict__ oz, uint32_t c0,
@@ -155,24 +198,26 @@ __global__ void __launch_bounds__(kBoundThreads) group_bound_kernel(const uint64
       t[W + w] = oz[static_cast<size_t>(i) * W + w];
     }
     uint32_t found = G0;
-    for (uint32_t g0 = 0; g0 < G0; g0 += 32) {
-      const uint32_t g = g0 + lane;
-      bool ok = false;
-      if (g < G0) {
-        if (FULL) {
-          ok = members_commute<W>(t, ox, oz, next, first[g]);
-        } else {
+    if (FULL) {
+      // found by group_search_full_kernel (UINT_MAX: no group accepts)
+      found = min(lb[i], G0);
+    } else {
+      for (uint32_t g0 = 0; g0 < G0; g0 += 32) {
+        const uint32_t g = g0 + lane;
+        bool ok = false;
+        if (g < G0) {
           uint64_t r[2 * W];
           load_row<W>(rows + static_cast<size_t>(g) * (2 * W), r);
           ok = row_accepts<W>(t, r);
         }
-      }
-      const unsigned b = __ballot_sync(0xffffffffu, ok);
-      if (b) {
-        found = g0 + __ffs(b) - 1;
-        break;
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (b) {
+          found = g0 + __ffs(b) - 1;
+          break;
+        }
       }
     }
+    __syncwarp();
     if (lane == 0) lb[i] = found;
     if (FULL) {
       // which of the 32 groups from the bound accept the term now
@@ -429,6 +474,14 @@ void run_greedy(int device, bool full, const uint64_t* ox, const uint64_t* oz, u
   for (uint32_t c0 = 0; c0 < T; c0 += chunk) {
     const uint32_t c1 = T - c0 > chunk ? c0 + chunk : T;
     const unsigned blocks = std::min<unsigned>(max_blocks, (c1 - c0 + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
+    if (full) {
+      wg::check_cuda(cudaMemsetAsync(lb + c0, 0xff, 4 * static_cast<size_t>(c1 - c0), s), "clear bounds");
+      const unsigned sblocks = std::min<unsigned>(
+          max_blocks, ((c1 - c0) * kBoundSplit + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
+      WG_TIMED("group_search_full_kernel", s,
+        group_search_full_kernel<W><<<sblocks, kBoundThreads, 0, s>>>(ox, oz, c0, c1, first, next, ng, lb));
+      wg::check_launch("launch group bound search");
+    }
     WG_TIMED("group_bound_kernel", s,
       kb<<<blocks, kBoundThreads, 0, s>>>(ox, oz, c0, c1, rows, first, next, ng, lb, lbm));
     wg::check_launch("launch group bounds");
