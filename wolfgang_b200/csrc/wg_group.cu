@@ -73,10 +73,11 @@ __global__ void gather_terms_kernel(const uint64_t* __restrict__ x, const uint64
 // next[pos] member lists in processing order; the bound pass also records
 // which of the 32 groups from the bound accepted the term at the chunk's start
 // (lbm), so that those need checking only against the chunk's own members.
-// Chunk lengths, measured on config 3: qwc 1,024 (512: 88 ms, 1,024: 81 ms,
-// 2,048: 122 ms for 262,144 terms); full mode 96 (64: 88 ms, 96: 79 ms, 128:
-// 81 ms, 256: 114 ms, 512: 213 ms for 32,768 terms), where every failed bound
-// costs member-list walks and shorter chunks keep the bounds closer.
+// Chunk lengths, measured on random 128-qubit terms (each qubit non-identity
+// with probability 0.05): qwc 1,024 (512: 88 ms, 1,024: 81 ms, 2,048: 122 ms
+// for 262,144 terms); full mode 96 (64: 88 ms, 96: 79 ms, 128: 81 ms, 256:
+// 114 ms, 512: 213 ms for 32,768 terms), where every failed bound costs
+// member-list walks and shorter chunks keep the bounds closer.
 constexpr int kChunk = 1024;     // terms per chunk (qwc); also the staging capacity
 constexpr int kChunkFull = 96;   // terms per chunk in full mode
 constexpr int kBoundThreads = 256;
