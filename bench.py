@@ -53,7 +53,10 @@ def peaks() -> tuple[float, str]:
 # ---------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """nvidia-smi samples every 200 ms while the timed region runs.  A region
+    shorter than the first sample gets one sample taken right after it (the
+    record then says so): a leftover clock lock or a throttle reason still
+    shows there."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -63,6 +66,7 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines: list[str] = []
+        self.after_region = False
 
     def __enter__(self):
         try:
@@ -81,6 +85,11 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            if not self.lines:
+                self.after_region = True
+                deadline = time.time() + 2.0
+                while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                    time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -103,7 +112,7 @@ class ClockSampler:
                 if flag.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "sampled_after_region": self.after_region}
 
 
 # ---------------------------------------------------------------- distributed
