@@ -225,9 +225,9 @@ def reference_products_sample(A, B, rows: int) -> tuple[float, int]:
 
 def bench_products(args, world, rank, torch) -> dict:
     from wolfgang_b200 import capi
-    from wolfgang_b200.workloads import config2
+    from wolfgang_b200.workloads import klocal_pair_100q
 
-    A, B = config2(args.lhs_terms, args.rhs_terms)
+    A, B = klocal_pair_100q(args.lhs_terms, args.rhs_terms)
     n = A[0]
     W = 2
     nl, nr = len(A[3]), len(B[3])
@@ -410,9 +410,9 @@ def timed_steps(torch, steps, warmup, fn, flush=None):
 def bench_commutation(args, world, rank, torch) -> dict:
     """Config 3: bit-packed 262,144^2 commutation matrix (128 qubits)."""
     from wolfgang_b200 import capi
-    from wolfgang_b200.workloads import config3
+    from wolfgang_b200.workloads import sparse_operator_128q
 
-    n, x, z, _ = config3(args.terms)
+    n, x, z, _ = sparse_operator_128q(args.terms)
     T = len(x)
     pitch = (T + 31) // 32
     dx, dz = dev(torch, x), dev(torch, z)
@@ -453,9 +453,9 @@ def bench_commutation(args, world, rank, torch) -> dict:
 def bench_grouping(args, world, rank, torch) -> dict:
     """Config 3, second half: group_commuting of the 262,144-term operator (mode qwc, or full)."""
     from wolfgang_b200 import capi
-    from wolfgang_b200.workloads import config3
+    from wolfgang_b200.workloads import sparse_operator_128q
 
-    n, x, z, c = config3(args.terms)
+    n, x, z, c = sparse_operator_128q(args.terms)
     T = len(x)
     dx, dz = dev(torch, x), dev(torch, z)
     order = np.zeros(T, np.uintp)
@@ -496,10 +496,10 @@ def bench_grouping(args, world, rank, torch) -> dict:
 def bench_expectation(args, world, rank, torch) -> dict:
     """Config 4: 26 qubits (1 GiB psi), 20,000 Hermitian terms in 2,000 x-groups; E + dE/dc + dE/dpsi*."""
     from wolfgang_b200.expectation import ExpectationPlan
-    from wolfgang_b200.workloads import config4_operator
+    from wolfgang_b200.workloads import xpattern_operator
 
     n = args.qubits
-    op = config4_operator(n=n)
+    op = xpattern_operator(n=n)
     g = torch.Generator(device="cuda")
     g.manual_seed(20261207)
     psi = torch.randn(1 << n, dtype=torch.complex128, device="cuda", generator=g)
@@ -549,15 +549,15 @@ def bench_expectation(args, world, rank, torch) -> dict:
 def bench_batched(args, world, rank, torch) -> dict:
     """Config 5: 512 uneven (H, psi) pairs, forward + gradient, batched vs per-call."""
     from wolfgang_b200.expectation import ExpectationBatch, ExpectationPlan
-    from wolfgang_b200.workloads import config5_operator, config5_pairs
+    from wolfgang_b200.workloads import uneven_pair_operator, uneven_pairs
 
-    pairs = config5_pairs(args.pairs)
+    pairs = uneven_pairs(args.pairs)
     if world > 1:
         pairs = shard(pairs, rank, world)
     plans, psis = [], []
     dtype = torch.complex64 if args.c64 else torch.complex128
     for n, T, seed in pairs:
-        plans.append(ExpectationPlan(config5_operator(n, T, seed)))
+        plans.append(ExpectationPlan(uneven_pair_operator(n, T, seed)))
         gen = torch.Generator(device="cuda")
         gen.manual_seed(seed)
         p = torch.randn(1 << n, dtype=torch.complex128, device="cuda", generator=gen)
@@ -582,13 +582,13 @@ def bench_batched(args, world, rank, torch) -> dict:
         # as T * 2^n * (time per amplitude at the nearest probed size)
         from oracle import Reference
 
-        from wolfgang_b200.workloads import config5_state
+        from wolfgang_b200.workloads import uneven_pair_state
 
         ref = Reference()
         probe = {}
         for n_probe in (12, 16, 20, 24):
-            op = config5_operator(n_probe, 64, 7 + n_probe)
-            st = config5_state(n_probe, 7 + n_probe)
+            op = uneven_pair_operator(n_probe, 64, 7 + n_probe)
+            st = uneven_pair_state(n_probe, 7 + n_probe)
             k = 64 if n_probe <= 20 else 4
             t0 = time.perf_counter()
             ref.expectation(n_probe, op[1][:k], op[2][:k], op[3][:k], st)
@@ -613,9 +613,9 @@ def bench_batched(args, world, rank, torch) -> dict:
 
 def reference_arm(args, world, rank) -> dict:
     """Times the reference's own CPU core on bounded samples of the same workload."""
-    from wolfgang_b200.workloads import config2
+    from wolfgang_b200.workloads import klocal_pair_100q
 
-    A, B = config2()
+    A, B = klocal_pair_100q()
     for _ in range(args.warmup):
         reference_products_sample(A, B, 16)
     total, prods = 0.0, 0

@@ -123,11 +123,11 @@ def test_bucket_klocal_products_match_lsd(cuda, oracle, algo):
     assert same(got, oracle.simplify(100, *raw, 1e-12, 0.0))
 
 
-def test_bucket_config1_hh_auto(cuda, oracle, algo):
-    """H@H of config 1 (2^24 products) takes the bucketed path by default."""
-    from wolfgang_b200.workloads import config1
+def test_bucket_hh_20q_operator_auto(cuda, oracle, algo):
+    """H@H of the 4,096-term 20-qubit operator (2^24 products) takes the bucketed path by default."""
+    from wolfgang_b200.workloads import hamiltonian_20q_and_state
 
-    (n, x, z, c), _ = config1()
+    (n, x, z, c), _ = hamiltonian_20q_and_state()
     algo(capi.WG_SORT_AUTO)
     got = G.products(n, (x, z, c), (x, z, c), capi.WG_PRODUCTS_SIMPLIFY)
     assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET

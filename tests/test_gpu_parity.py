@@ -46,10 +46,10 @@ def test_commutation_bits_match_oracle(cuda, oracle, algo, n, nl, nr):
         assert np.all(bits[:, -1] >> np.uint32(nr % 32) == 0)
 
 
-def test_commutation_algorithms_agree_on_config1(cuda):
-    from wolfgang_b200.workloads import config1
+def test_commutation_algorithms_agree_on_20q_operator(cuda):
+    from wolfgang_b200.workloads import hamiltonian_20q_and_state
 
-    (n, x, z, _), _ = config1()
+    (n, x, z, _), _ = hamiltonian_20q_and_state()
     b1 = G.commutation_bits(n, (x, z), (x, z), algo=1)
     b2 = G.commutation_bits(n, (x, z), (x, z), algo=2)
     assert same_bits(b1, b2)
@@ -74,10 +74,10 @@ def test_commutation_wide_tiles_match(cuda, oracle, n):
     assert np.all(b2[:, -1] >> np.uint32(nr % 32) == 0)
 
 
-def test_commutation_config3_row_slice_matches_oracle(cuda, oracle):
-    from wolfgang_b200.workloads import config3
+def test_commutation_128q_row_slice_matches_oracle(cuda, oracle):
+    from wolfgang_b200.workloads import sparse_operator_128q
 
-    n, x, z, _ = config3()
+    n, x, z, _ = sparse_operator_128q()
     rows = slice(0, 1024)
     bits = G.commutation_bits(n, (x[rows], z[rows]), (x, z), algo=0)
     want = oracle.commutes(n, (x[rows], z[rows]), (x, z))
@@ -222,10 +222,10 @@ def test_products_bit_exact(cuda, oracle, case, mode):
         assert same_bits(g, w)
 
 
-def test_config1_hh_simplify_bit_exact(cuda, oracle):
-    from wolfgang_b200.workloads import config1
+def test_hh_20q_operator_simplify_bit_exact(cuda, oracle):
+    from wolfgang_b200.workloads import hamiltonian_20q_and_state
 
-    (n, x, z, c), _ = config1()
+    (n, x, z, c), _ = hamiltonian_20q_and_state()
     got = G.products(n, (x, z, c), (x, z, c), capi.WG_PRODUCTS_SIMPLIFY)
     want = oracle.matmul(n, (x, z, c), (x, z, c), simplify=True)
     for g, w in zip(got, want):
@@ -272,10 +272,10 @@ def test_expectation_one_shot_and_zero_qubits(cuda, oracle):
     assert complex(out[0], out[1]) == pytest.approx(3.5 - 0.75j, abs=1e-15)
 
 
-def test_expectation_config1(cuda, oracle):
-    from wolfgang_b200.workloads import config1
+def test_expectation_20q_operator(cuda, oracle):
+    from wolfgang_b200.workloads import hamiltonian_20q_and_state
 
-    (n, x, z, c), psi = config1()
+    (n, x, z, c), psi = hamiltonian_20q_and_state()
     plan = G.Plan(n, x, z, c)
     E, _, _ = plan.run(G.dev(psi))
     assert abs(E - oracle.expectation(n, x, z, c, psi)) <= 1e-12

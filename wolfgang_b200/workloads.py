@@ -24,8 +24,9 @@ import numpy as np
 SEED_BASE = 20261203
 
 
-def rng_for(config: int) -> np.random.Generator:
-    return np.random.default_rng(SEED_BASE + config)
+def rng_for(k: int) -> np.random.Generator:
+    """Generator of workload k: PCG64 seeded with SEED_BASE + k."""
+    return np.random.default_rng(SEED_BASE + k)
 
 
 def words_for(n: int) -> int:
@@ -81,26 +82,26 @@ def random_state(rng: np.random.Generator, n: int, dtype=np.complex128) -> np.nd
     return psi.astype(dtype)
 
 
-def config1():
+def hamiltonian_20q_and_state():
     rng = rng_for(1)
     H = bernoulli_operator(rng, 20, 4096, 0.25)
     psi = random_state(rng, 20)
     return H, psi
 
 
-def config2(scale_a: int = 32768, scale_b: int = 16384):
+def klocal_pair_100q(scale_a: int = 32768, scale_b: int = 16384):
     rng = rng_for(2)
     A = klocal_operator(rng, 100, scale_a, np.array([2, 3, 4]))
     B = klocal_operator(rng, 100, scale_b, np.array([2, 3, 4]))
     return A, B
 
 
-def config3(T: int = 262144):
+def sparse_operator_128q(T: int = 262144):
     rng = rng_for(3)
     return bernoulli_operator(rng, 128, T, 0.05)
 
 
-def config4_operator(n: int = 26, T: int = 20000, patterns: int = 2000, seed_offset: int = 0):
+def xpattern_operator(n: int = 26, T: int = 20000, patterns: int = 2000, seed_offset: int = 0):
     """Hermitian H with x-masks from `patterns` distinct x-patterns."""
     rng = np.random.default_rng(SEED_BASE + 4 + seed_offset)
     pats: list[np.ndarray] = []
@@ -131,11 +132,11 @@ def config4_operator(n: int = 26, T: int = 20000, patterns: int = 2000, seed_off
     return n, x, z, c
 
 
-def config4_state(n: int = 26) -> np.ndarray:
+def state_26q(n: int = 26) -> np.ndarray:
     return random_state(np.random.default_rng(SEED_BASE + 40), n)
 
 
-def config5_pairs(count: int = 512, n_min: int = 8, n_max: int = 24, t_min: int = 100, t_max: int = 50000):
+def uneven_pairs(count: int = 512, n_min: int = 8, n_max: int = 24, t_min: int = 100, t_max: int = 50000):
     """List of (n, T, seed) descriptors; operators/states are built per pair."""
     rng = rng_for(5)
     ns = rng.integers(n_min, n_max + 1, size=count)
@@ -143,10 +144,10 @@ def config5_pairs(count: int = 512, n_min: int = 8, n_max: int = 24, t_min: int 
     return [(int(ns[i]), int(Ts[i]), SEED_BASE + 5000 + i) for i in range(count)]
 
 
-def config5_operator(n: int, T: int, seed: int):
+def uneven_pair_operator(n: int, T: int, seed: int):
     rng = np.random.default_rng(seed)
     return klocal_operator(rng, n, T, np.arange(1, min(6, n) + 1), real=True)
 
 
-def config5_state(n: int, seed: int, dtype=np.complex128) -> np.ndarray:
+def uneven_pair_state(n: int, seed: int, dtype=np.complex128) -> np.ndarray:
     return random_state(np.random.default_rng(seed + 1_000_000), n, dtype)
