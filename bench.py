@@ -636,7 +636,7 @@ def reference_arm(args, world, rank) -> dict:
     }
 
 
-def main() -> None:
+def build_parser() -> argparse.ArgumentParser:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -659,7 +659,11 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lhs-terms", type=int, default=32768, help="A terms (smaller values: profiling cases)")
     ap.add_argument("--rhs-terms", type=int, default=16384, help="B terms")
-    args = ap.parse_args()
+    return ap
+
+
+def main() -> None:
+    args = build_parser().parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
 
