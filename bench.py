@@ -43,6 +43,37 @@ PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 
 
+def load_workloads():
+    """The seeded workload generators (numpy only), loaded by file path:
+    importing them as wolfgang_b200.workloads would run the package's
+    __init__, which loads its native libraries -- the reference arm must not
+    map any of them."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("wg_bench_workloads", ROOT / "wolfgang_b200" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def host_cpu() -> dict:
+    """CPU model and the cores this process may run on (for every CPU baseline)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    return {"cpu_model": model, "nproc": usable}
+
+
 def peaks() -> tuple[float, str]:
     try:
         return float(json.loads(PEAKS_FILE.read_text())["hbm_gbs"]), "measured"
@@ -177,6 +208,24 @@ def shard(items: list, rank: int, world: int) -> list:
 
 
 # ---------------------------------------------------------------- helpers
+
+def pinned_d2h_bandwidth(torch, nbytes: int = 1 << 30) -> float:
+    """Device-to-pinned-host copy bandwidth of this box in GB/s (best of 3
+    copies of 1 GiB, CUDA events): the link that bounds an end-to-end call
+    whose result comes back to the host."""
+    src = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    best = float("inf")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del src, dst
+    return nbytes / (best * 1e-3) / 1e9
+
 
 def flush_l2(torch, buf):
     buf.add_(1.0)  # 512 MiB write, larger than the 126 MB L2
@@ -335,6 +384,8 @@ def bench_products(args, world, rank, torch) -> dict:
         fits = avail is None or avail >= local_ranks * result_bytes * 1.3
         concurrent = max_over_ranks(0.0 if fits else 1.0, world) == 0.0
 
+        step_s: list[float] = []
+
         def e2e_calls() -> tuple[float, int]:
             r = hA.matmul(hB, max_intermediate_terms=P)  # warm
             t0 = time.perf_counter()
@@ -342,8 +393,10 @@ def bench_products(args, world, rank, torch) -> dict:
                 # each step is one call: the previous step's result is released
                 # first (inside the timed region), so that a call does not run
                 # beside another 24 GB result
+                ts = time.perf_counter()
                 r = None
                 r = hA.matmul(hB, max_intermediate_terms=P)
+                step_s.append(time.perf_counter() - ts)
             dt_, terms_ = (time.perf_counter() - t0) / args.e2e_steps, r.num_terms
             del r
             return dt_, terms_
@@ -360,6 +413,9 @@ def bench_products(args, world, rank, torch) -> dict:
             barrier(world)
         dt = max_over_ranks(dt, world)
         out["e2e"] = {"value": world * P / dt, "unit": "terms/s", "s_per_step": dt,
+                      "steps": args.e2e_steps, "s_per_step_min": min(step_s) if step_s else None,
+                      "s_per_step_max": max(step_s) if step_s else None,
+                      "pinned_d2h_GBps": pinned_d2h_bandwidth(torch),
                       "h2d_bytes_per_step": (nl + nr) * (16 * W + 16),
                       "d2h_bytes_per_step": terms * (16 * W + 16),
                       "api": "wolfgang_quantum.PauliSum.matmul (host operands and result)",
@@ -371,8 +427,11 @@ def bench_products(args, world, rank, torch) -> dict:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         secs, prods = reference_products_sample(A, B, args.cpu_rows)
         out["cpu_baseline"] = {"value": prods / secs, "unit": "terms/s", "cores": 1, "kind": "reference",
+                               "extrapolated": True, **host_cpu(),
                                "sample": f"A[:{args.cpu_rows}] x B = {prods} products, reference PauliSum::matmul"
-                                         f"(simplify=True) compiled from its sources, {secs:.1f} s"}
+                                         f"(simplify=True) compiled from its sources, {secs:.1f} s; products/s of "
+                                         "the row sample stand for the full A x B (every lhs row meets the same "
+                                         "rhs); the reference's matmul and simplify are single-threaded"}
     return out
 
 
@@ -445,7 +504,7 @@ def bench_commutation(args, world, rank, torch) -> dict:
         ref.commutes(n, (x[:rows], z[:rows]), (x, z))
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": rows * T / dt, "unit": "pairs/s", "cores": 1, "kind": "reference",
-                               "sample": f"{rows} rows x {T} terms via reference PauliSum::commutes_with "
+                               "extrapolated": True, **host_cpu(), "sample": f"{rows} rows x {T} terms via reference PauliSum::commutes_with "
                                          f"(auto CPU dispatch: {ref.cpu_backend()}), {dt:.1f} s"}
     return out
 
@@ -487,7 +546,7 @@ def bench_grouping(args, world, rank, torch) -> dict:
         groups = Reference().group_commuting(n, x[:rows], z[:rows], c[:rows], mode=args.group_mode)
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": rows / dt, "unit": "terms/s", "cores": 1, "kind": "reference",
-                               "sample": f"reference PauliSum::group_commuting(mode={args.group_mode!r}) on the first "
+                               "extrapolated": rows < T, **host_cpu(), "sample": f"reference PauliSum::group_commuting(mode={args.group_mode!r}) on the first "
                                          f"{rows} terms ({len(groups)} groups, {dt:.1f} s); the greedy's cost grows "
                                          "with the number of open groups, so the full operator runs slower per term"}
     return out
@@ -534,7 +593,7 @@ def bench_expectation(args, world, rank, torch) -> dict:
         Reference().expectation(n, x, z, c, hpsi)
         per_term = (time.perf_counter() - t0) / k
         out_cpu = {"value": 1.0 / (per_term * len(op[3])), "unit": "evals/s", "cores": 1, "kind": "reference",
-                   "sample": f"reference expectation_statevector_complex128 on the first {k} of {len(op[3])} terms "
+                   "extrapolated": True, **host_cpu(), "sample": f"reference expectation_statevector_complex128 on the first {k} of {len(op[3])} terms "
                              f"({per_term:.3f} s per term), scaled to all terms; forward only (no gradient in "
                              f"the reference)"}
     return {"metric": "E+grad evals/s" if not args.forward_only else "E evals/s", "value": world * 1e3 / t,
@@ -598,7 +657,7 @@ def bench_batched(args, world, rank, torch) -> dict:
 
         est = sum(T * per_amp(n) * (1 << n) for n, T, _ in pairs)
         cpu = {"value": len(pairs) / est, "unit": "evals/s", "cores": 1, "kind": "reference",
-               "sample": "reference expectation_statevector_complex128 timed per term at 12/16/20/24 qubits "
+               "extrapolated": True, **host_cpu(), "sample": "reference expectation_statevector_complex128 timed per term at 12/16/20/24 qubits "
                          f"({', '.join(f'{q}: {v * 1e9:.2f} ns/amp' for q, v in probe.items())}); every pair "
                          "estimated as T * 2^n * (ns per amplitude at the nearest probed size); forward only (no gradient in the "
                          f"reference); {est:.0f} s estimated for the batch"}
@@ -612,10 +671,11 @@ def bench_batched(args, world, rank, torch) -> dict:
 
 
 def reference_arm(args, world, rank) -> dict:
-    """Times the reference's own CPU core on bounded samples of the same workload."""
-    from wolfgang_b200.workloads import klocal_pair_100q
+    """Times the reference's own CPU core on bounded samples of the same workload.
 
-    A, B = klocal_pair_100q()
+    Only oracle/_ref/libwgref.so (the reference core compiled from its sources)
+    is loaded: the generators come in by file path, not through the package."""
+    A, B = load_workloads().klocal_pair_100q()
     for _ in range(args.warmup):
         reference_products_sample(A, B, 16)
     total, prods = 0.0, 0
@@ -629,9 +689,14 @@ def reference_arm(args, world, rank) -> dict:
         "ms_per_step": 1e3 * total / args.steps,
         "config": {"workload": "config2: A(32768)xB(16384) terms, 100 qubits, k-local w in {2,3,4}, matmul+simplify(atol=1e-12)",
                    "sample_rows": args.ref_rows},
-        "cpu_baseline": {"value": v, "unit": "terms/s", "cores": 1, "kind": "reference",
+        "extrapolated": True,
+        "cpu_baseline": {"value": v, "unit": "terms/s", "cores": 1, "kind": "reference", "extrapolated": True,
+                         **host_cpu(),
                          "sample": f"A[:{args.ref_rows}] x B per step ({args.ref_rows * len(B[3])} products), "
-                                   "reference PauliSum::matmul(simplify=True), scalar path, 1 core"},
+                                   "reference PauliSum::matmul(simplify=True), scalar path; products/s of the row "
+                                   "sample stand for the full A(32768) x B(16384) (every lhs row meets the same "
+                                   "rhs); the reference's matmul and simplify are single-threaded, so 1 core of "
+                                   "nproc is used"},
         "e2e": {"value": v, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -652,7 +717,7 @@ def build_parser() -> argparse.ArgumentParser:
     ap.add_argument("--c64", action="store_true", help="complex64 statevector storage")
     ap.add_argument("--forward-only", action="store_true")
     ap.add_argument("--pairs", type=int, default=512, help="batched pairs (config 5)")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--cpu-terms", type=int, default=8, help="reference terms timed for the expectation baseline")
     ap.add_argument("--ref-rows", type=int, default=256)

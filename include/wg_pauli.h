@@ -66,9 +66,14 @@ int wg_memcpy_dtod(int device, void* dst, const void* src, size_t bytes, wg_stre
  * shorter).  Lets a caller build its own host container from the data without
  * first filling it (e.g. appending to a reserved std::vector).  Calls from
  * different threads run concurrently, each with its own staging and stream.
+ * Ordering: the copies run on an internal stream that first waits for all
+ * work enqueued on `stream` before the call (pass the stream whose kernels
+ * write src; NULL = the legacy default stream).  Work enqueued on other
+ * streams is not waited for.  Returns once every chunk has been handed over.
  * No reference counterpart (the reference downloads into resized vectors). */
 typedef void (*wg_chunk_fn)(void* user, const void* chunk, size_t chunk_bytes);
-int wg_memcpy_dtoh_chunked(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user);
+int wg_memcpy_dtoh_chunked(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user,
+                           wg_stream_t stream);
 int wg_memset(int device, void* dst, int value, size_t bytes, wg_stream_t stream);
 int wg_stream_synchronize(int device, wg_stream_t stream);
 int wg_device_synchronize(int device);

@@ -309,6 +309,19 @@ class Reference:
                                                _p(_ptr(psi)), ctypes.c_int(dtype), _p(_ptr(out))))
         return complex(out[0], out[1])
 
+    def expectation_z_counts(self, n, x, z, c, packed, counts) -> complex:
+        T = len(c)
+        w = words_for(n)
+        x, z, c = _u64(x, T, w), _u64(z, T, w), _c128(c, T)
+        rows = len(counts)
+        packed = np.ascontiguousarray(np.asarray(packed, np.uint64).reshape(rows, w))
+        counts = np.ascontiguousarray(np.asarray(counts, np.float64))
+        out = np.zeros(2, np.float64)
+        self._check(self.lib.wgref_expectation_z_counts(_sz(n), _sz(T), _sz(w), _p(_ptr(x)), _p(_ptr(z)),
+                                                        _p(_ptr(c)), _sz(rows), _p(_ptr(packed)),
+                                                        _p(_ptr(counts)), _p(_ptr(out))))
+        return complex(out[0], out[1])
+
     def cpu_backend(self) -> str:
         buf = ctypes.create_string_buffer(512)
         self._check(self.lib.wgref_cpu_backend(buf, _sz(512)))

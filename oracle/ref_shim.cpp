@@ -144,6 +144,25 @@ int wgref_expectation(size_t n, size_t T, size_t words, const uint64_t* x,
   });
 }
 
+// PauliSum::expectation_z_counts with the bitstrings given packed (row-major,
+// `words` words per row, qubit q = bit q%64 of word q/64); they are written
+// back out as the reference's strings, whose first character is qubit n-1.
+int wgref_expectation_z_counts(size_t n, size_t T, size_t words, const uint64_t* x,
+                               const uint64_t* z, const double* c, size_t rows,
+                               const uint64_t* packed, const double* counts, double* out) {
+  return guarded([&] {
+    const auto op = make_sum(n, T, words, x, z, c);
+    std::vector<std::string> bitstrings(rows, std::string(n, '0'));
+    for (size_t r = 0; r < rows; ++r)
+      for (size_t q = 0; q < n; ++q)
+        if ((packed[r * words + q / 64] >> (q % 64)) & 1U) bitstrings[r][n - 1 - q] = '1';
+    const std::vector<double> cnt(counts, counts + rows);
+    const std::complex<double> v = op.expectation_z_counts(bitstrings, cnt);
+    out[0] = v.real();
+    out[1] = v.imag();
+  });
+}
+
 // Reports the CPU dispatch the reference would use for commutes_with in this
 // process: the active backend and the candidates' availability.
 int wgref_cpu_backend(char* buf, size_t cap) {

@@ -7,8 +7,9 @@ sources (``make -C oracle``):
 
 Each fixture stores seeded inputs and the reference's outputs for one case:
 simplify, matmul (raw, simplified, fused path), commutation flags,
-group_commuting (qwc and full) and expectation values (complex128 and
-complex64, general and all-diagonal).  tests/test_golden.py checks the
+group_commuting (qwc and full), expectation values (complex128 and
+complex64, general and all-diagonal) and Z-count expectations.  Names given
+on the command line limit the run to those fixtures.  tests/test_golden.py checks the
 oracle against them and tests/test_gpu_golden.py the device kernels.
 """
 
@@ -101,9 +102,25 @@ def main() -> None:
         e = ref.expectation(n, x, z, c, psi)
         out[name] = dict(n=np.int64(n), x=x, z=z, c=c, psi=psi, value=np.complex128(e))
 
-    for name, arrays in out.items():
-        np.savez_compressed(HERE / f"{name}.npz", **arrays)
-    print("wrote", len(out), "fixtures to", HERE)
+    for name, (seed, n, T, p, rows) in {"zcounts_w1": (50, 10, 60, 0.3, 300),
+                                        "zcounts_w2": (51, 100, 40, 0.05, 500)}.items():
+        _, x, z, c = op(seed, n, T, p)
+        x[:] = 0  # Z-count expectations take diagonal terms only
+        rng = np.random.default_rng(seed + 9)
+        w = (n + 63) // 64
+        bits = rng.random((rows, n)) < 0.5
+        padded = np.zeros((rows, 64 * w), np.uint8)
+        padded[:, :n] = bits
+        packed = np.packbits(padded, axis=1, bitorder="little").view("<u8").reshape(rows, w).astype(np.uint64)
+        counts = rng.integers(0, 50, size=rows).astype(np.float64)
+        e = ref.expectation_z_counts(n, x, z, c, packed, counts)
+        out[name] = dict(n=np.int64(n), x=x, z=z, c=c, packed=packed, counts=counts, value=np.complex128(e))
+
+    only = set(sys.argv[1:])
+    written = [name for name in out if not only or name in only]
+    for name in written:
+        np.savez_compressed(HERE / f"{name}.npz", **out[name])
+    print("wrote", len(written), "fixtures to", HERE)
 
 
 if __name__ == "__main__":

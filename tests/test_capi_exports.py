@@ -96,6 +96,6 @@ def test_bucket_fine_target_is_range_checked_before_device_work():
 
 def test_chunked_download_needs_a_callback():
     L = capi.lib()
-    rc = L.wg_memcpy_dtoh_chunked(0, None, 64, None, None)
+    rc = L.wg_memcpy_dtoh_chunked(0, None, 64, None, None, None)
     assert rc == capi.WG_ERR_INVALID and b"callback" in L.wg_last_error()
-    assert L.wg_memcpy_dtoh_chunked(0, None, 0, None, None) == capi.WG_OK
+    assert L.wg_memcpy_dtoh_chunked(0, None, 0, None, None, None) == capi.WG_OK

@@ -63,3 +63,10 @@ def test_group_golden(oracle, name, mode):
 def test_expectation_golden(oracle, name):
     g = load(name)
     assert oracle.expectation(int(g["n"]), g["x"], g["z"], g["c"], g["psi"]) == complex(g["value"])
+
+
+@pytest.mark.parametrize("name", ["zcounts_w1", "zcounts_w2"])
+def test_z_counts_golden(oracle, name):
+    g = load(name)
+    got = oracle.expectation_z_counts(int(g["n"]), g["x"], g["z"], g["c"], g["packed"], g["counts"])
+    assert got == complex(g["value"])

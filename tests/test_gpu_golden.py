@@ -69,3 +69,20 @@ def test_expectation_golden_on_device(cuda, name, tol):
     capi.call("wg_expectation", 0, int(g["n"]), len(g["c"]), dx.data_ptr(), dz.data_ptr(), dc.data_ptr(),
               psi.data_ptr(), dtype, out, None)
     assert abs(complex(out[0], out[1]) - complex(g["value"])) <= tol
+
+
+
+@pytest.mark.parametrize("name", ["zcounts_w1", "zcounts_w2"])
+def test_z_counts_golden_on_device(cuda, name):
+    """wg_expectation_z_counts on the device against the reference core's value
+    (packed bitstrings; the weighted sums of integer counts are exact, so the
+    result is compared within 1e-12)."""
+    g = load(name)
+    n = int(g["n"])
+    w = (n + 63) // 64
+    out = (ctypes.c_double * 2)()
+    dx, dz, dc = G.operator_on_device(g["x"], g["z"], g["c"])
+    dp, dn = G.dev(g["packed"]), G.dev(g["counts"])
+    capi.call("wg_expectation_z_counts", 0, w, len(g["c"]), dx.data_ptr(), dz.data_ptr(), dc.data_ptr(),
+              len(g["counts"]), dp.data_ptr(), dn.data_ptr(), out, None)
+    assert abs(complex(out[0], out[1]) - complex(g["value"])) <= 1e-12

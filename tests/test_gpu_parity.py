@@ -198,6 +198,9 @@ MATMUL_CASES = [
     (100, 2048, 1024, 0.03, None, None),
     (150, 60, 70, 0.03, None, None),
     (0, 5, 6, 0.0, None, None),
+    # more than eight mask words (the any-width products kernel)
+    (600, 40, 50, 0.01, None, None),
+    (1000, 30, 20, 0.01, 10, None),
 ]
 
 
@@ -311,7 +314,11 @@ def test_z_counts_match_oracle(cuda, oracle):
                                         (200, 5000, 0.03, None), (256, 2500, 0.02, None),
                                         # dense terms: about one qwc group per term, more groups than
                                         # shared memory holds (the bases stay in global memory)
-                                        (128, 8000, 0.5, None)])
+                                        (128, 8000, 0.5, None),
+                                        # more than four mask words: the any-width kernels (5, 11 and
+                                        # 40 words; at 40 words a qwc chunk stages 356 terms)
+                                        (300, 3000, 0.02, None), (300, 1500, 0.2, 600),
+                                        (700, 2500, 0.01, None), (2560, 400, 0.003, None)])
 def test_group_commuting_matches_oracle(cuda, oracle, mode, n, T, p, pool):
     import ctypes
 

@@ -137,3 +137,38 @@ def test_term_expectations_and_hpsi_are_consistent(oracle):
     assert abs(np.dot(c, e) - E) < 1e-11
     hp = oracle.hpsi(n, x, z, c, psi)
     assert abs(np.vdot(psi, hp) - E) < 1e-11
+
+
+@pytest.mark.parametrize("n,T,rows", [(1, 2, 3), (7, 40, 100), (64, 30, 257), (65, 25, 90), (130, 12, 40)])
+def test_z_counts_match_reference(oracle, reference, n, T, rows):
+    """expectation_z_counts (src/expectation.cpp:219-247): the oracle takes the
+    bitstrings packed, the reference as strings (first character = qubit n-1);
+    the shim converts between them."""
+    rng = np.random.default_rng(1000 + n * 7 + rows)
+    _, x, z, c = random_operator(rng, n, T, 0.3)
+    x[:] = 0
+    w = (n + 63) // 64
+    packed = rng.integers(0, 2**63, size=(rows, w), dtype=np.uint64)
+    if n % 64:
+        packed[:, -1] &= np.uint64((1 << (n % 64)) - 1)
+    counts = rng.integers(0, 20, size=rows).astype(np.float64)
+    counts[0] += 1.0  # a positive total
+    assert oracle.expectation_z_counts(n, x, z, c, packed, counts) == reference.expectation_z_counts(
+        n, x, z, c, packed, counts)
+
+
+def test_z_counts_errors_match_reference(oracle, reference):
+    from oracle import OracleError
+
+    rng = np.random.default_rng(3)
+    n, x, z, c = random_operator(rng, 6, 5, 0.5)
+    packed = np.zeros((2, 1), np.uint64)
+    for bad_x, counts, msg in [(True, np.array([1.0, 2.0]), "diagonal"), (False, np.array([-1.0, 2.0]), "non-negative"),
+                               (False, np.array([0.0, 0.0]), "positive"), (False, np.array([np.inf, 1.0]), "finite")]:
+        xx = x.copy() if bad_x else np.zeros_like(x)
+        if bad_x:
+            xx[0, 0] |= np.uint64(1)
+        with pytest.raises(OracleError, match=msg):
+            oracle.expectation_z_counts(n, xx, z, c, packed, counts)
+        with pytest.raises(OracleError, match=msg):
+            reference.expectation_z_counts(n, xx, z, c, packed, counts)

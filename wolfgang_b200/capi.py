@@ -51,7 +51,7 @@ _SIGNATURES: dict[str, list] = {
     "wg_memcpy_htod": [_i, _vp, _vp, _sz, _vp],
     "wg_memcpy_dtoh": [_i, _vp, _vp, _sz, _vp],
     "wg_memcpy_dtod": [_i, _vp, _vp, _sz, _vp],
-    "wg_memcpy_dtoh_chunked": [_i, _vp, _sz, _vp, _vp],
+    "wg_memcpy_dtoh_chunked": [_i, _vp, _sz, _vp, _vp, _vp],
     "wg_memset": [_i, _vp, _i, _sz, _vp],
     "wg_stream_synchronize": [_i, _vp],
     "wg_device_synchronize": [_i],

@@ -23,6 +23,24 @@ inline void check(int status) {
   throw std::runtime_error(msg);
 }
 
+// Commutation algorithm for wg_commutation_bits when the caller holds the lhs
+// terms on the host: the mean lhs weight (set qubits) over up to 256 rows,
+// read from host memory, decides between the ballot kernel (1), whose cost is
+// ~32 (4W + 2) instructions per output word whatever the weight, and the
+// bit-plane kernel (2), ~8 per set bit + 16.  Without host terms the library's
+// own size rule (algo 0) applies.
+inline int commutation_algo_for(std::size_t words, const std::uint64_t* x, const std::uint64_t* z,
+                                std::size_t n_lhs, std::size_t n_rhs) {
+  if (words == 0 || words > 4 || n_rhs < 512 || n_lhs < 64) return 0;
+  const std::size_t sample = n_lhs < 256 ? n_lhs : 256;
+  std::size_t weight = 0;
+  for (std::size_t i = 0; i < sample * words; ++i) weight += __builtin_popcountll(x[i] | z[i]);
+  const double mean_w = static_cast<double>(weight) / static_cast<double>(sample);
+  const double ballot_cost = 32.0 * (4.0 * static_cast<double>(words) + 2.0);
+  const double plane_cost = 8.0 * mean_w + 16.0;
+  return plane_cost < ballot_cost ? 2 : 1;
+}
+
 class DeviceBuffer {
  public:
   DeviceBuffer() = default;
@@ -74,7 +92,7 @@ class DeviceBuffer {
       const T* b = static_cast<const T*>(chunk);
       out->insert(out->end(), b, b + bytes / sizeof(T));
     };
-    check(wg_memcpy_dtoh_chunked(device_, ptr_, count * sizeof(T), fn, &v));
+    check(wg_memcpy_dtoh_chunked(device_, ptr_, count * sizeof(T), fn, &v, nullptr));
   }
   template <typename T>
   T* as() const {

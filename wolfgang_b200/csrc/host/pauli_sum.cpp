@@ -383,9 +383,10 @@ std::vector<std::uint8_t> PauliSum::commutes_with(const PauliSum& rhs,
   DeviceOperand l = upload(dev, *this), r = upload(dev, rhs);
   const std::size_t pitch = (rhs.num_terms_ + 31) / 32;
   DeviceBuffer bits(dev, num_terms_ * pitch * 4), flags(dev, entries);
+  const int algo = abi::commutation_algo_for(words_, x_.data(), z_.data(), num_terms_, rhs.num_terms_);
   abi::check(wg_commutation_bits(dev, words_, l.x.as<std::uint64_t>(), l.z.as<std::uint64_t>(), num_terms_,
                                  r.x.as<std::uint64_t>(), r.z.as<std::uint64_t>(), rhs.num_terms_,
-                                 bits.as<std::uint32_t>(), pitch, 0, nullptr));
+                                 bits.as<std::uint32_t>(), pitch, algo, nullptr));
   abi::check(wg_bits_to_u8(dev, bits.as<std::uint32_t>(), num_terms_, rhs.num_terms_, pitch,
                            flags.as<std::uint8_t>(), nullptr));
   flags.download(out.data(), entries);

@@ -179,8 +179,9 @@ constexpr size_t kStagedMin = size_t{32} << 20;
 bool pinned_host(const void* p);
 void staged_copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
 // Device-to-host copy through a pinned staging pair of its own; fn gets each
-// chunk in order on the calling thread.
-void chunked_download(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user);
+// chunk in order on the calling thread.  The copies start after all work
+// enqueued on `after` so far.
+void chunked_download(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user, cudaStream_t after);
 
 // Per-device grow-only workspace for an entry point's intermediates.  It is
 // held for the whole call (calls on one device take turns on it) and kept for

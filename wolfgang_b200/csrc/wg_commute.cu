@@ -134,6 +134,7 @@ __global__ void fill_ones_kernel(uint32_t* bits, size_t rows, size_t cols, size_
 // consecutive output words of a row (read as one LW-word vector per plane):
 // LW = 4 with 1,024 threads for large products of 1-2 mask words (planes take
 // up to 128 KB of shared memory), LW = 2 with 256 threads otherwise.
+constexpr int kMaxConfiguredDevices = 64;
 constexpr int kRowList = 16;  // plane offsets listed per row; rows with more set bits loop over their masks
 
 template <int LW>
@@ -309,12 +310,14 @@ void launch_plane_as(const uint64_t* lx, const uint64_t* lz, size_t n_l, const u
   constexpr int kWordsCta = 32 * LW;
   auto* kernel = commute_plane_kernel<W, LW, THREADS>;
   const size_t smem = static_cast<size_t>(64 * W) * 2 * kWordsCta * sizeof(uint32_t);
-  static bool configured[64] = {};
-  if (!configured[device & 63]) {
+  // The shared-memory opt-in is per device and per kernel; set once per device
+  // (std::call_once also orders host threads that launch concurrently).
+  static std::once_flag configured[kMaxConfiguredDevices];
+  if (device < 0 || device >= kMaxConfiguredDevices) wg::throw_invalid("CUDA device ordinal is out of range");
+  std::call_once(configured[device], [&] {  // a throw leaves the flag unset: the next call retries
     wg::check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                    "configure bit-plane commutation");
-    configured[device & 63] = true;
-  }
+  });
   const size_t col_blocks = (n_r + 32 * kWordsCta - 1) / (32 * kWordsCta);
   // Enough row chunks to fill the machine (at least four CTAs per SM); as many
   // rows per CTA as that allows, to amortise the plane building: on 262,144^2
@@ -353,25 +356,23 @@ void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint
   launch_plane_as<W, 2, 256>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
 }
 
-// Autotuned choice between the two algorithms.  Cost model per output word:
-//   ballot: 32 pairs * (4W LOP3 + 1 POPC)  (compute; ~independent of weight)
-//   plane : mean lhs weight smem XORs (+ plane build per CTA)
-// The mean weight is estimated from a sample of lhs rows on the host side of
-// the launch (read back from the device: 256 rows at most).
-int choose_algo(size_t W, const uint64_t* lx, const uint64_t* lz, size_t n_l, size_t n_r,
-                cudaStream_t s) {
+// Default choice between the two algorithms, from the sizes and the word
+// count alone: it reads no term data, so it costs no device-to-host copy and
+// no synchronisation, and a call that uses it can be captured in a CUDA graph.
+// Cost model per output word:
+//   ballot: 32 pairs * (4W LOP3 + 1 POPC + pack)  ~ 32 * (4W + 2) instructions
+//   plane : about 8 per set bit of the lhs row (find bit, offsets, 16-byte
+//           shared load, XORs) + 16, plus the plane tile built once per CTA.
+// The plane kernel wins up to a mean lhs weight of (32(4W+2) - 16) / 8, i.e.
+// 22 set qubits at one word and 38 at two: every workload of this path's
+// benchmark set is far below that (k-local and sparse operators of weight
+// 2-8).  Small products keep the ballot kernel (no tile to amortise).  Callers
+// that know the weight pass algo 1 or 2 themselves (the C++ layer estimates it
+// from its host copy of the terms), and the autotuner's cached measurement
+// replaces this rule for shape classes it has searched.
+int default_algo(size_t W, size_t n_l, size_t n_r) {
   if (W > 4 || n_r < 512 || n_l < 64) return 1;
-  const size_t sample = n_l < 256 ? n_l : 256;
-  std::vector<uint64_t> hx(sample * W), hz(sample * W);
-  wg::check_cuda(cudaMemcpyAsync(hx.data(), lx, hx.size() * 8, cudaMemcpyDeviceToHost, s), "sample lhs");
-  wg::check_cuda(cudaMemcpyAsync(hz.data(), lz, hz.size() * 8, cudaMemcpyDeviceToHost, s), "sample lhs");
-  wg::check_cuda(cudaStreamSynchronize(s), "sample lhs");
-  size_t weight = 0;
-  for (size_t i = 0; i < hx.size(); ++i) weight += __builtin_popcountll(hx[i] | hz[i]);
-  const double mean_w = static_cast<double>(weight) / static_cast<double>(sample);
-  const double ballot_cost = 32.0 * (4.0 * W + 2.0);  // instructions per output word
-  const double plane_cost = 8.0 * mean_w + 16.0;        // per output word
-  return plane_cost < ballot_cost ? 2 : 1;
+  return 2;
 }
 
 }  // namespace
@@ -394,7 +395,7 @@ int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x, const u
       wg::check_launch("launch commutation fill");
       return;
     }
-    if (algo == 0) algo = choose_algo(words, lhs_x, lhs_z, n_lhs, n_rhs, s);
+    if (algo == 0) algo = default_algo(words, n_lhs, n_rhs);
     if (algo == 2 && words <= 4) {
       switch (words) {
         case 1: launch_plane<1>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;

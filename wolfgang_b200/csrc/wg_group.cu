@@ -492,6 +492,275 @@ void run_greedy(int device, bool full, const uint64_t* ox, const uint64_t* oz, u
   }
 }
 
+// ------------------------------------------------ any number of mask words
+// More than 4 mask words (over 256 qubits): the same chunked first-fit as
+// above, with each row read word by word from memory instead of held in
+// registers.  Term rows are interleaved once as trows[i] = [x words | z words]
+// (processing order); a chunk's term rows are staged in shared memory, the
+// qwc basis rows and the full-mode member lists stay in global memory.  The
+// chunk is shortened when its staged rows would not fit in shared memory.
+
+__device__ __forceinline__ bool row_accepts_n(const uint64_t* t, const uint64_t* b, int W) {
+  uint64_t d = 0;
+  for (int w = 0; w < W; ++w) d |= (t[w] & b[W + w]) ^ (t[W + w] & b[w]);
+  return d == 0;
+}
+
+// parity of the symplectic product of two [x | z] rows
+__device__ __forceinline__ bool anticommutes_n(const uint64_t* t, const uint64_t* row, int W) {
+  uint64_t acc = 0;
+  for (int w = 0; w < W; ++w) acc ^= (t[w] & row[W + w]) ^ (t[W + w] & row[w]);
+  return (__popcll(acc) & 1u) != 0;
+}
+
+__device__ __forceinline__ bool members_commute_n(const uint64_t* t, const uint64_t* __restrict__ trows,
+                                                  const uint32_t* next, uint32_t m, int W) {
+  for (; m != UINT_MAX; m = next[m])
+    if (anticommutes_n(t, trows + static_cast<size_t>(m) * (2 * W), W)) return false;
+  return true;
+}
+
+__global__ void interleave_rows_kernel(const uint64_t* __restrict__ ox, const uint64_t* __restrict__ oz, size_t T,
+                                       int W, uint64_t* __restrict__ trows) {
+  const size_t n = T * static_cast<size_t>(W);
+  for (size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; k < n;
+       k += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t i = k / W, w = k - i * W;
+    trows[i * (2 * W) + w] = ox[k];
+    trows[i * (2 * W) + W + w] = oz[k];
+  }
+}
+
+// group_search_full_kernel for any width
+__global__ void __launch_bounds__(kBoundThreads) group_search_full_n_kernel(
+    const uint64_t* __restrict__ trows, int W, uint32_t c0, uint32_t c1, const uint32_t* __restrict__ first,
+    const uint32_t* __restrict__ next, const uint32_t* __restrict__ n_groups, uint32_t* lb) {
+  const uint32_t G0 = *n_groups;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t units = (c1 - c0) * kBoundSplit;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < units; u += nw) {
+    const uint32_t i = c0 + u / kBoundSplit, sub = u % kBoundSplit;
+    const uint64_t* t = trows + static_cast<size_t>(i) * (2 * W);
+    for (uint32_t g0 = sub * 32; g0 < G0; g0 += 32 * kBoundSplit) {
+      uint32_t best = 0;
+      if (lane == 0) best = *static_cast<volatile uint32_t*>(&lb[i]);
+      best = __shfl_sync(0xffffffffu, best, 0);
+      if (g0 >= best) break;
+      const uint32_t g = g0 + lane;
+      const bool ok = g < G0 && members_commute_n(t, trows, next, first[g], W);
+      const unsigned b = __ballot_sync(0xffffffffu, ok);
+      if (b) {
+        if (lane == 0) atomicMin(&lb[i], g0 + __ffs(b) - 1);
+        break;
+      }
+    }
+  }
+}
+
+// group_bound_kernel for any width
+__global__ void __launch_bounds__(kBoundThreads) group_bound_n_kernel(
+    const uint64_t* __restrict__ trows, int W, uint32_t c0, uint32_t c1, const uint64_t* __restrict__ rows,
+    const uint32_t* __restrict__ first, const uint32_t* __restrict__ next, const uint32_t* __restrict__ n_groups,
+    uint32_t* __restrict__ lb, uint32_t* __restrict__ lbm, int full) {
+  const uint32_t G0 = *n_groups;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < c1; i += nw) {
+    const uint64_t* t = trows + static_cast<size_t>(i) * (2 * W);
+    uint32_t found = G0;
+    if (full) {
+      found = min(lb[i], G0);
+    } else {
+      for (uint32_t g0 = 0; g0 < G0; g0 += 32) {
+        const uint32_t g = g0 + lane;
+        const bool ok = g < G0 && row_accepts_n(t, rows + static_cast<size_t>(g) * (2 * W), W);
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (b) {
+          found = g0 + __ffs(b) - 1;
+          break;
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) lb[i] = found;
+    if (full) {
+      const uint32_t g = found + lane;
+      const bool ok = g < G0 && members_commute_n(t, trows, next, first[g], W);
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (lane == 0) lbm[i] = m;
+    }
+  }
+}
+
+// place_qwc for any width, basis rows in global memory (lane g % 32 owns row g)
+__device__ uint32_t place_qwc_n(const uint64_t* st, const uint32_t* slb, uint32_t* sgid, uint32_t n, uint32_t G,
+                                uint64_t* B, int W) {
+  const uint32_t lane = threadIdx.x & 31;
+  const size_t rw = 2 * static_cast<size_t>(W);
+  uint32_t k = 0;
+  while (k < n) {
+    uint32_t l = 0;
+    for (; k < n; ++k) {
+      const uint64_t* t = st + k * rw;
+      l = slb[k];
+      const uint32_t g = l + ((lane - l) & 31u);
+      const bool ok = g < G && row_accepts_n(t, B + g * rw, W);
+      const uint32_t best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+      if (best == UINT_MAX) break;
+      if (best % 32 == lane)
+        for (size_t e = 0; e < rw; ++e) B[best * rw + e] |= t[e];
+      if (lane == 0) sgid[k] = best;
+    }
+    if (k >= n) break;
+    const uint64_t* t = st + k * rw;
+    uint32_t best = UINT_MAX;
+    for (uint32_t g0 = l + 32; best == UINT_MAX && g0 < G; g0 += 32) {
+      const uint32_t g = g0 + ((lane - g0) & 31u);
+      const bool ok = g < G && row_accepts_n(t, B + g * rw, W);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    const bool fresh = best == UINT_MAX;
+    if (fresh) best = G;
+    if (best % 32 == lane)
+      for (size_t e = 0; e < rw; ++e) B[best * rw + e] = fresh ? t[e] : (B[best * rw + e] | t[e]);
+    if (fresh) ++G;
+    if (lane == 0) sgid[k] = best;
+    ++k;
+  }
+  return G;
+}
+
+// place_full for any width
+__device__ uint32_t place_full_n(const uint64_t* __restrict__ trows, const uint64_t* st, const uint32_t* slb,
+                                 const uint32_t* smask, uint32_t* sgid, uint32_t n, uint32_t c0, uint32_t G0,
+                                 uint32_t* first, uint32_t* last, uint32_t* next, int W) {
+  const uint32_t lane = threadIdx.x & 31;
+  const size_t rw = 2 * static_cast<size_t>(W);
+  uint32_t G = G0;
+  auto chunk_members_commute = [&](const uint64_t* t, uint32_t g, uint32_t k) {
+    for (uint32_t q = 0; q < k; ++q)
+      if (sgid[q] == g && anticommutes_n(t, st + q * rw, W)) return false;
+    return true;
+  };
+  auto place = [&](uint32_t k, uint32_t best, bool fresh) {
+    if ((k & 31u) == lane) sgid[k] = best;
+    if (lane == 0) {
+      const uint32_t i = c0 + k;
+      next[i] = UINT_MAX;
+      if (fresh) first[best] = i;
+      else next[last[best]] = i;
+      last[best] = i;
+    }
+  };
+  uint32_t k = 0;
+  while (k < n) {
+    uint32_t l = 0;
+    for (; k < n; ++k) {
+      const uint64_t* t = st + k * rw;
+      l = slb[k];
+      if (l >= G0) break;
+      bool bad = false;
+      for (uint32_t q = lane; q < k; q += 32)
+        if (sgid[q] == l && anticommutes_n(t, st + q * rw, W)) bad = true;
+      if (__any_sync(0xffffffffu, bad)) break;
+      place(k, l, false);
+    }
+    if (k >= n) break;
+    __syncwarp();
+    const uint64_t* t = st + k * rw;
+    const uint32_t m = smask[k];
+    uint32_t best = UINT_MAX;
+    {
+      const uint32_t g = l + lane;
+      const bool ok = l < G0 && lane > 0 && g < G0 && ((m >> lane) & 1u) && chunk_members_commute(t, g, k);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    for (uint32_t g0 = l + 32; best == UINT_MAX && g0 < G0; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      const bool ok = g < G0 && members_commute_n(t, trows, next, first[g], W);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    for (uint32_t g0 = G0; best == UINT_MAX && g0 < G; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      const bool ok = g < G && chunk_members_commute(t, g, k);
+      best = __reduce_min_sync(0xffffffffu, ok ? g : UINT_MAX);
+    }
+    const bool fresh = best == UINT_MAX;
+    if (fresh) best = G;
+    place(k, best, fresh);
+    if (fresh) ++G;
+    __syncwarp();
+    ++k;
+  }
+  return G;
+}
+
+// group_resolve_kernel for any width: stages up to `cap_terms` term rows
+__global__ void __launch_bounds__(kResolveThreads) group_resolve_n_kernel(
+    const uint64_t* __restrict__ trows, int W, uint32_t c0, uint32_t c1, uint32_t cap_terms, uint64_t* rows,
+    uint32_t* first, uint32_t* last, uint32_t* next, const uint32_t* __restrict__ lb,
+    const uint32_t* __restrict__ lbm, uint32_t* __restrict__ group_of, uint32_t* __restrict__ n_groups, int full) {
+  extern __shared__ __align__(16) unsigned char nraw[];
+  const size_t rw = 2 * static_cast<size_t>(W);
+  const uint32_t n = c1 - c0;
+  uint64_t* st = reinterpret_cast<uint64_t*>(nraw);
+  uint32_t* slb = reinterpret_cast<uint32_t*>(st + static_cast<size_t>(cap_terms) * rw);
+  uint32_t* sgid = slb + cap_terms;
+  uint32_t* smask = sgid + cap_terms;
+  const uint32_t G0 = *n_groups;
+  for (size_t k = threadIdx.x; k < n * rw; k += blockDim.x) st[k] = trows[static_cast<size_t>(c0) * rw + k];
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    slb[k] = lb[c0 + k];
+    if (full) smask[k] = lbm[c0 + k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const uint32_t G = full ? place_full_n(trows, st, slb, smask, sgid, n, c0, G0, first, last, next, W)
+                            : place_qwc_n(st, slb, sgid, n, G0, rows, W);
+    if (threadIdx.x == 0) *n_groups = G;
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) group_of[c0 + k] = sgid[k];
+}
+
+void run_greedy_n(int device, bool full, int W, const uint64_t* trows, uint32_t T, uint64_t* rows, uint32_t* first,
+                  uint32_t* last, uint32_t* next, uint32_t* lb, uint32_t* lbm, uint32_t* gid, uint32_t* ng,
+                  cudaStream_t s) {
+  const auto& props = wg::device_props(device);
+  const size_t per_term = 16 * static_cast<size_t>(W) + 12;  // staged row, bound, group id, bound mask
+  const size_t smem_max = static_cast<size_t>(props.max_smem_optin);
+  const uint32_t want = full ? kChunkFull : kChunk;
+  const uint32_t chunk = static_cast<uint32_t>(std::min<size_t>(want, smem_max / per_term));
+  if (chunk == 0) wg::throw_invalid("group_commuting: a term row does not fit in shared memory");
+  const size_t smem = static_cast<size_t>(chunk) * per_term;
+  wg::check_cuda(cudaFuncSetAttribute(group_resolve_n_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)),
+                 "set group resolve shared memory");
+  wg::check_cuda(cudaMemsetAsync(ng, 0, 4, s), "clear group count");
+  const unsigned max_blocks = static_cast<unsigned>(props.sm_count) * 8;
+  for (uint32_t c0 = 0; c0 < T; c0 += chunk) {
+    const uint32_t c1 = T - c0 > chunk ? c0 + chunk : T;
+    const unsigned blocks = std::min<unsigned>(max_blocks, (c1 - c0 + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
+    if (full) {
+      wg::check_cuda(cudaMemsetAsync(lb + c0, 0xff, 4 * static_cast<size_t>(c1 - c0), s), "clear bounds");
+      const unsigned sblocks = std::min<unsigned>(
+          max_blocks, ((c1 - c0) * kBoundSplit + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
+      WG_TIMED("group_search_full_n_kernel", s,
+        group_search_full_n_kernel<<<sblocks, kBoundThreads, 0, s>>>(trows, W, c0, c1, first, next, ng, lb));
+      wg::check_launch("launch group bound search");
+    }
+    WG_TIMED("group_bound_n_kernel", s,
+      group_bound_n_kernel<<<blocks, kBoundThreads, 0, s>>>(trows, W, c0, c1, rows, first, next, ng, lb, lbm,
+                                                            full ? 1 : 0));
+    wg::check_launch("launch group bounds");
+    WG_TIMED("group_resolve_n_kernel", s,
+      group_resolve_n_kernel<<<1, kResolveThreads, smem, s>>>(trows, W, c0, c1, chunk, rows, first, last, next, lb,
+                                                              lbm, gid, ng, full ? 1 : 0));
+    wg::check_launch("launch group resolve");
+  }
+}
+
 // ---------------------------------------------------------------- Z counts
 
 __global__ void or_reduce_kernel(const uint64_t* __restrict__ v, size_t n, unsigned long long* __restrict__ out) {
@@ -556,7 +825,6 @@ int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t*
     *n_groups = 0;
     if (n_terms == 0) return;
     if (n_terms >= 0xffffffffull) wg::throw_invalid("group_commuting supports fewer than 2^32-1 terms");
-    if (words > 4) wg::throw_invalid("group_commuting on the device supports at most 256 qubits");
     wg::DeviceGuard g(device);
     cudaStream_t s = stream;
     const size_t T = n_terms;
@@ -583,6 +851,13 @@ int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t*
         gid(4 * T, s), ng(4, s);
     const bool full = mode_full != 0;
     const uint32_t T32 = static_cast<uint32_t>(T);
+    wg::Scratch trows(W > 4 ? 16 * Wa * T : 0, s);
+    if (W > 4) {
+      WG_TIMED("interleave_rows_kernel", s,
+        interleave_rows_kernel<<<wg::grid_for(T * W, kThreads, device, 4), kThreads, 0, s>>>(
+            ox.as<uint64_t>(), oz.as<uint64_t>(), T, W, trows.as<uint64_t>()));
+      wg::check_launch("launch interleave rows");
+    }
     switch (W) {
       case 0:
       case 1: run_greedy<1>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
@@ -597,10 +872,13 @@ int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t*
                                first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
                                lbm.as<uint32_t>(), gid.as<uint32_t>(),
                                ng.as<uint32_t>(), s); break;
-      default: run_greedy<4>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                                first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
+      case 4: run_greedy<4>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
+                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
                                lbm.as<uint32_t>(), gid.as<uint32_t>(),
-                                ng.as<uint32_t>(), s); break;
+                               ng.as<uint32_t>(), s); break;
+      default: run_greedy_n(device, full, W, trows.as<uint64_t>(), T32, rows.as<uint64_t>(), first.as<uint32_t>(),
+                            last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(), lbm.as<uint32_t>(),
+                            gid.as<uint32_t>(), ng.as<uint32_t>(), s); break;
     }
     uint32_t G = 0;
     wg::check_cuda(cudaMemcpyAsync(&G, ng.get(), 4, cudaMemcpyDeviceToHost, s), "read group count");

@@ -172,6 +172,7 @@ void parallel_memcpy(char* dst, const char* src, size_t bytes) {
 struct ChunkStage {
   void* buf[2] = {nullptr, nullptr};
   cudaEvent_t done[2] = {nullptr, nullptr};
+  cudaEvent_t ready = nullptr;  // recorded on the caller's stream: src is complete
   cudaStream_t stream = nullptr;
   int device = -1;
 };
@@ -196,12 +197,14 @@ ChunkStage* take_chunk_stage(int device) {
       check_cuda(cudaHostAlloc(&c->buf[i], kStageBytes, cudaHostAllocPortable), "allocate pinned staging");
       check_cuda(cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming), "create staging event");
     }
+    check_cuda(cudaEventCreateWithFlags(&c->ready, cudaEventDisableTiming), "create staging event");
     check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "create staging stream");
   } catch (...) {
     for (int i = 0; i < 2; ++i) {
       if (c->buf[i]) (void)cudaFreeHost(c->buf[i]);
       if (c->done[i]) (void)cudaEventDestroy(c->done[i]);
     }
+    if (c->ready) (void)cudaEventDestroy(c->ready);
     delete c;
     throw;
   }
@@ -214,12 +217,17 @@ void give_chunk_stage(ChunkStage* c) {
 }
 }  // namespace
 
-void chunked_download(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user) {
+void chunked_download(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user, cudaStream_t after) {
   ChunkStage* c = take_chunk_stage(device);
   const char* const sp = static_cast<const char*>(src);
   const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
   auto len_of = [&](size_t k) { return std::min(kStageBytes, bytes - k * kStageBytes); };
   try {
+    // The staging stream is a non-blocking stream of its own: order its copies
+    // after everything already enqueued on the caller's stream (the work that
+    // writes src), or they could read src before that work has finished.
+    check_cuda(cudaEventRecord(c->ready, after), "record download order");
+    check_cuda(cudaStreamWaitEvent(c->stream, c->ready, 0), "order download after the caller's stream");
     // DMA chunk k into buffer k%2 while the caller consumes chunk k-1
     for (size_t k = 0; k <= chunks; ++k) {
       if (k < chunks) {
@@ -434,12 +442,13 @@ int wg_memcpy_dtoh(int device, void* dst, const void* src, size_t bytes, wg_stre
   });
 }
 
-int wg_memcpy_dtoh_chunked(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user) {
+int wg_memcpy_dtoh_chunked(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user,
+                           wg_stream_t stream) {
   return guarded([&] {
     if (bytes == 0) return;
     if (fn == nullptr) throw_invalid("chunked download needs a chunk callback");
     DeviceGuard g(device);
-    wg::chunked_download(device, src, bytes, fn, user);
+    wg::chunked_download(device, src, bytes, fn, user, stream);
   });
 }
 

@@ -76,8 +76,6 @@ __device__ __forceinline__ void product_term(const uint64_t* __restrict__ lx, co
   c = wgd::rotate(wgd::cmul(a, b), e);
 }
 
-constexpr int kMaxW = 8;
-
 template <int W>
 __global__ void __launch_bounds__(kThreads) products_kernel(
     const uint64_t* __restrict__ lx, const uint64_t* __restrict__ lz, const double* __restrict__ lc, size_t n_l,
@@ -91,8 +89,29 @@ __global__ void __launch_bounds__(kThreads) products_kernel(
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const size_t l = p / n_r;
     const size_t r = p - l * n_r;
-    uint64_t px[kMaxW], pz[kMaxW];
     c128 c;
+    if constexpr (W < 0) {
+      // any width: each word's product is stored as soon as it is formed
+      unsigned e = 0;
+      for (int w = 0; w < WW; ++w) {
+        const uint64_t ax = __ldg(lx + l * WW + w), az = __ldg(lz + l * WW + w);
+        const uint64_t bx = __ldg(rx + r * WW + w), bz = __ldg(rz + r * WW + w);
+        const uint64_t px = ax ^ bx, pz = az ^ bz;
+        e += __popcll(px & pz) - __popcll(ax & az) - __popcll(bx & bz) + 2u * __popcll(ax & bz);
+        if (keys) {
+          keys[(2 * w) * P + p] = px;
+          keys[(2 * w + 1) * P + p] = pz;
+        } else {
+          out_x[p * WW + w] = px;
+          out_z[p * WW + w] = pz;
+        }
+      }
+      const c128 a{__ldg(lc + 2 * l), __ldg(lc + 2 * l + 1)};
+      const c128 b{__ldg(rc + 2 * r), __ldg(rc + 2 * r + 1)};
+      c = wgd::rotate(wgd::cmul(a, b), e);
+      if (keys) idx[p] = static_cast<uint32_t>(p);
+    } else {
+    uint64_t px[W > 0 ? W : 1], pz[W > 0 ? W : 1];
     product_term<W>(lx, lz, lc, rx, rz, rc, l, r, Wrt, px, pz, c);
     if (keys) {
       for (int w = 0; w < WW; ++w) {
@@ -105,6 +124,7 @@ __global__ void __launch_bounds__(kThreads) products_kernel(
         out_x[p * WW + w] = px[w];
         out_z[p * WW + w] = pz[w];
       }
+    }
     }
     out_c[2 * p] = c.re;
     out_c[2 * p + 1] = c.im;
@@ -445,7 +465,6 @@ void products_dispatch(int W, const uint64_t* lx, const uint64_t* lz, const doub
     case 1: launch_products<1>(lx, lz, lc, n_l, rx, rz, rc, n_r, 1, keys, idx, ox, oz, oc, max_bits, device, s); break;
     case 2: launch_products<2>(lx, lz, lc, n_l, rx, rz, rc, n_r, 2, keys, idx, ox, oz, oc, max_bits, device, s); break;
     default:
-      if (W > kMaxW) wg::throw_invalid("matmul supports at most 512 qubits on the device");
       launch_products<-1>(lx, lz, lc, n_l, rx, rz, rc, n_r, W, keys, idx, ox, oz, oc, max_bits, device, s);
   }
 }
