@@ -348,6 +348,58 @@ def test_device_commutation_outputs():
         da.commutes_with_device(db, output=DeviceCommutationMatrix.empty((2, 2)))
 
 
+def test_device_commutation_matrix_dlpack():
+    """DeviceCommutationMatrix.__dlpack__ (reference .pyi:29-30,
+    bindings/python/pauli_sum_py.cpp:663-821): a read-only view of the dense
+    uint8 buffer that torch imports without a copy, lifetime-tied to the
+    matrix, with the reference's refusals."""
+    import gc
+
+    import torch
+
+    rng = np.random.default_rng(12)
+    letters = np.array(list("IXYZ"))
+    a = PauliSum.from_labels(["".join(rng.choice(letters, 7)) for _ in range(31)])
+    b = PauliSum.from_labels(["".join(rng.choice(letters, 7)) for _ in range(45)])
+    want = a.commutes_with(b)
+    m = a.to_device().commutes_with_device(b.to_device())
+    assert m.__dlpack_device__() == (2, 0)
+    t = torch.from_dlpack(m)
+    assert t.dtype == torch.uint8 and tuple(t.shape) == (31, 45) and t.device == torch.device("cuda", 0)
+    assert t.data_ptr() == m.__cuda_array_interface__["data"][0]  # a view of the matrix, not a copy
+    np.testing.assert_array_equal(t.cpu().numpy().astype(bool), want)
+    np.testing.assert_array_equal(t.cpu().numpy().astype(bool), m.to_host())
+    # the view keeps the buffer alive after the matrix object is dropped
+    del m
+    gc.collect()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(t.cpu().numpy().astype(bool), want)
+
+    m = a.to_device().commutes_with_device(b.to_device())
+    cap = m.__dlpack__(max_version=(1, 0))  # an unconsumed capsule is freed with it
+    del cap
+    gc.collect()
+    with pytest.raises(BufferError, match="copy=True"):
+        m.__dlpack__(max_version=(1, 0), copy=True)
+    with pytest.raises(BufferError, match=r"max_version >= \(1, 0\)"):
+        m.__dlpack__()
+    with pytest.raises(BufferError, match=r"max_version >= \(1, 0\)"):
+        m.__dlpack__(max_version=(0, 8))
+    with pytest.raises(ValueError, match="stream=0 is ambiguous"):
+        m.__dlpack__(stream=0, max_version=(1, 0))
+    with pytest.raises(ValueError, match="non-negative"):
+        m.__dlpack__(stream=-1, max_version=(1, 0))
+    with pytest.raises(TypeError, match="stream must be None or an integer"):
+        m.__dlpack__(stream="s", max_version=(1, 0))
+    with pytest.raises(ValueError, match=r"\(major, minor\) tuple"):
+        m.__dlpack__(max_version=(1,))
+    with pytest.raises(ValueError, match="uint32"):
+        m.__dlpack__(max_version=(-1, 0))
+    # an explicit copy through torch is allowed (torch copies after importing the view)
+    c = torch.from_dlpack(m, copy=False)
+    assert c.data_ptr() == m.__cuda_array_interface__["data"][0]
+
+
 def test_device_errors():
     d = PauliSum.from_labels(["XX"]).to_device()
     with pytest.raises(ValueError, match="same num_qubits"):

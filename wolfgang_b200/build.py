@@ -83,6 +83,20 @@ def _common_deps() -> list[Path]:
     return [CSRC / h for h in CU_HEADERS] + [INCLUDE / "wg_pauli.h"]
 
 
+def _dlpack_include() -> str:
+    """Directory holding ATen/dlpack.h, the DLPack C ABI header that torch
+    ships (a standalone C header; the module includes nothing else of torch)."""
+    import importlib.util
+
+    spec = importlib.util.find_spec("torch")
+    if spec is None or not spec.submodule_search_locations:
+        raise RuntimeError("torch's include directory (for ATen/dlpack.h) was not found")
+    inc = Path(list(spec.submodule_search_locations)[0]) / "include"
+    if not (inc / "ATen" / "dlpack.h").exists():
+        raise RuntimeError(f"ATen/dlpack.h not found under {inc}")
+    return str(inc)
+
+
 def build(verbose: bool = False, jobs: int | None = None) -> Path:
     """Compile everything that is out of date; return the Python module path."""
     if not Path(NVCC).exists() and shutil.which("nvcc") is None:
@@ -128,7 +142,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     msrc = HOST / "module.cpp"
     if _stale(mod, [msrc, wolfgang] + host_deps):
         _run([CXX, *CXX_FLAGS, "-shared", "-o", str(mod), str(msrc),
-              "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+              "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"], "-I", _dlpack_include(),
               f"-L{LIB}", "-lwolfgang", "-lwgpauli", "-Wl,-rpath,$ORIGIN/lib", *SHARED_LINK])
     if verbose:
         print(f"built {wgpauli}, {wolfgang}, {mod}")

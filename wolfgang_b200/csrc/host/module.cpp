@@ -16,10 +16,12 @@
 #include <complex>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <span>
 #include <string>
 #include <vector>
 
+#include "ATen/dlpack.h"  // the DLPack C ABI (a plain C header shipped with torch; no torch code)
 #include "wg_pauli.h"
 #include "wolfgang/device_pauli_sum.hpp"
 #include "wolfgang/pauli_sum.hpp"
@@ -277,6 +279,128 @@ AcceleratorBackend backend_arg(const py::object& b) {
 
 py::object axis_counts(const std::vector<std::uint64_t>& v) { return u64_array(v); }
 
+// ------------------------------------------------------------- DLPack export
+// DeviceCommutationMatrix.__dlpack__ keeps the reference's contract
+// (bindings/python/pauli_sum_py.cpp:663-821, .pyi:29-30): a versioned,
+// read-only capsule "dltensor_versioned" of the dense (rows, cols) uint8
+// buffer, compact row-major; the consumer's max_version must be at least
+// (1, 0) (a legacy capsule cannot carry the read-only flag) and the producer
+// answers with the lower of it and the version it was built against;
+// copy=True and stream=0 are refused.  The capsule holds a reference to the
+// Python matrix object, so the buffer lives as long as any view of it.  The
+// buffer is complete when exported (every call that writes it synchronises),
+// so no stream ordering is needed: a stream token is only validated.
+
+[[noreturn]] void buffer_error(const std::string& m) {
+  PyErr_SetString(PyExc_BufferError, m.c_str());
+  throw py::error_already_set();
+}
+
+struct MatrixDlpackContext {
+  std::unique_ptr<std::int64_t[]> shape;
+  std::unique_ptr<std::int64_t[]> strides;
+  PyObject* owner = nullptr;  // strong reference to the exporting matrix
+};
+
+void matrix_dlpack_deleter(DLManagedTensorVersioned* managed) {
+  if (managed == nullptr) return;
+  auto* ctx = static_cast<MatrixDlpackContext*>(managed->manager_ctx);
+  if (ctx != nullptr) {
+    if (ctx->owner != nullptr) {
+      PyGILState_STATE st = PyGILState_Ensure();  // consumers may call the deleter without the GIL
+      Py_DECREF(ctx->owner);
+      PyGILState_Release(st);
+    }
+    delete ctx;
+  }
+  delete managed;
+}
+
+// A capsule that no consumer took ("used_dltensor_versioned" once consumed)
+// frees its tensor when it is collected.
+void matrix_dlpack_capsule_destructor(PyObject* capsule) {
+  if (PyCapsule_IsValid(capsule, "used_dltensor_versioned")) return;
+  if (!PyCapsule_IsValid(capsule, "dltensor_versioned")) {
+    PyErr_Clear();
+    return;
+  }
+  auto* managed = static_cast<DLManagedTensorVersioned*>(PyCapsule_GetPointer(capsule, "dltensor_versioned"));
+  if (managed != nullptr && managed->deleter != nullptr) managed->deleter(managed);
+  else PyErr_Clear();
+}
+
+py::object matrix_dlpack(py::object self, py::object stream, py::object max_version, py::object copy,
+                         py::object dl_device) {
+  const auto& mtx = self.cast<const DeviceCommutationMatrix&>();
+  // dl_device (DLPack >= 2023.12 consumers): only the matrix's own device
+  if (!dl_device.is_none()) {
+    py::tuple own = py::make_tuple(mtx.dlpack_device_type(), mtx.device());
+    if (!dl_device.equal(own)) buffer_error("DeviceCommutationMatrix.__dlpack__ exports only on its own device");
+  }
+  if (!copy.is_none()) {
+    const int truth = PyObject_IsTrue(copy.ptr());
+    if (truth == 1) buffer_error("DeviceCommutationMatrix.__dlpack__ does not support copy=True");
+    PyErr_Clear();
+  }
+  if (!stream.is_none()) {
+    if (!PyLong_Check(stream.ptr())) type_error("stream must be None or an integer accelerator stream token");
+    const long long token = stream.cast<long long>();
+    if (token == 0) value_error("stream=0 is ambiguous in the Python DLPack protocol");
+    if (token < 0) value_error("stream must be non-negative");
+  }
+  // consumer's highest version; None leaves no read-only capable version
+  std::uint32_t major = 0, minor = 0;
+  if (!max_version.is_none()) {
+    if (!PyTuple_Check(max_version.ptr()) || PyTuple_Size(max_version.ptr()) != 2)
+      value_error("max_version must be None or a (major, minor) tuple");
+    py::tuple t = py::reinterpret_borrow<py::tuple>(max_version);
+    long long a = 0, b = 0;
+    try {
+      a = t[0].cast<long long>();
+      b = t[1].cast<long long>();
+    } catch (const py::cast_error&) {
+      value_error("max_version must be None or a (major, minor) tuple");
+    }
+    if (a < 0 || b < 0 || a > std::numeric_limits<std::uint32_t>::max() ||
+        b > std::numeric_limits<std::uint32_t>::max())
+      value_error("max_version components must be non-negative uint32 values");
+    major = static_cast<std::uint32_t>(a);
+    minor = static_cast<std::uint32_t>(b);
+  }
+  if (max_version.is_none() || major < 1)
+    buffer_error("DeviceCommutationMatrix.__dlpack__ requires max_version >= (1, 0) "
+                 "so the read-only DLPack contract can be represented");
+  DLPackVersion version{DLPACK_MAJOR_VERSION, DLPACK_MINOR_VERSION};
+  if (major < version.major || (major == version.major && minor < version.minor)) version = {major, minor};
+
+  auto ctx = std::make_unique<MatrixDlpackContext>();
+  ctx->shape = std::make_unique<std::int64_t[]>(2);
+  ctx->strides = std::make_unique<std::int64_t[]>(2);
+  ctx->shape[0] = static_cast<std::int64_t>(mtx.rows());
+  ctx->shape[1] = static_cast<std::int64_t>(mtx.cols());
+  ctx->strides[0] = static_cast<std::int64_t>(mtx.cols());
+  ctx->strides[1] = 1;
+  auto managed = std::make_unique<DLManagedTensorVersioned>();
+  managed->version = version;
+  managed->manager_ctx = ctx.get();
+  managed->deleter = &matrix_dlpack_deleter;
+  managed->flags = DLPACK_FLAG_BITMASK_READ_ONLY;
+  managed->dl_tensor.data = reinterpret_cast<void*>(mtx.data_pointer_for_dlpack());
+  managed->dl_tensor.device = DLDevice{static_cast<DLDeviceType>(mtx.dlpack_device_type()), mtx.device()};
+  managed->dl_tensor.ndim = 2;
+  managed->dl_tensor.dtype = DLDataType{static_cast<std::uint8_t>(kDLUInt), 8, 1};
+  managed->dl_tensor.shape = ctx->shape.get();
+  managed->dl_tensor.strides = ctx->strides.get();
+  managed->dl_tensor.byte_offset = 0;
+  PyObject* capsule = PyCapsule_New(managed.get(), "dltensor_versioned", &matrix_dlpack_capsule_destructor);
+  if (capsule == nullptr) throw py::error_already_set();
+  ctx->owner = self.ptr();
+  Py_INCREF(ctx->owner);
+  ctx.release();
+  managed.release();
+  return py::reinterpret_steal<py::object>(capsule);
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_wolfgang_core, m) {
@@ -336,6 +460,11 @@ PYBIND11_MODULE(_wolfgang_core, m) {
             value_error("axis must be None, 0, or 1");
           },
           py::arg("axis") = py::none())
+      .def("__dlpack__", &matrix_dlpack, py::arg("stream") = py::none(), py::arg("max_version") = py::none(),
+           py::arg("copy") = py::none(), py::arg("dl_device") = py::none(),
+           "Read-only DLPack capsule of the dense (rows, cols) uint8 device buffer (DLPack >= 1.0).")
+      .def("__dlpack_device__",
+           [](const DeviceCommutationMatrix& mtx) { return py::make_tuple(mtx.dlpack_device_type(), mtx.device()); })
       .def_property_readonly("__cuda_array_interface__", [](const DeviceCommutationMatrix& mtx) {
         py::dict d;
         d["shape"] = py::make_tuple(mtx.rows(), mtx.cols());
