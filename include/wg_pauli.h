@@ -171,6 +171,43 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
                       double rtol, uint64_t** out_x, uint64_t** out_z,
                       double** out_coeffs, size_t* out_terms, wg_stream_t stream);
 
+/* Prepared batch of products (new; no reference counterpart -- the per-call
+ * path it replaces is wg_pauli_products, i.e. matmul_product_kernel +
+ * simplify of src/cuda/matmul_cuda.cu:91-147, once per pair): n_pairs
+ * products lhs_p * rhs_p of uneven sizes, all with `words` mask words, each
+ * with PauliSum::matmul(simplify) semantics -- mode WG_PRODUCTS_SIMPLIFY
+ * (simplify(atol, rtol) per pair) or WG_PRODUCTS_FUSED (cull at 1e-12).
+ * Create reads the operands' masks once: it sorts every pair's products by
+ * key, groups equal keys in nested-loop order and sizes all scratch and the
+ * outputs (one slot per distinct key of a pair); it synchronises the device.
+ * wg_products_batch_run then only enqueues kernels on `stream` -- no
+ * allocation, host copy or host synchronisation -- so a run can be captured
+ * in a CUDA graph and replayed.  Each run reads the coefficients through the
+ * lhs_c/rhs_c device pointers given at create (their values may change
+ * between runs; the masks must not) and writes pair p's simplified product,
+ * in canonical order, to the batch's output slots (wg_products_batch_result)
+ * and its term count to the device array of wg_products_batch_counts.  At
+ * most 2^30 products per pair and fewer than 2^32 in all; runs of one batch
+ * must not overlap. */
+typedef struct wg_products_batch_s* wg_products_batch_t;
+int wg_products_batch_create(int device, size_t words, size_t n_pairs, const uint64_t* const* lhs_x,
+                             const uint64_t* const* lhs_z, const double* const* lhs_c, const size_t* n_lhs,
+                             const uint64_t* const* rhs_x, const uint64_t* const* rhs_z,
+                             const double* const* rhs_c, const size_t* n_rhs, int mode, double atol, double rtol,
+                             wg_products_batch_t* batch, wg_stream_t stream);
+int wg_products_batch_run(wg_products_batch_t batch, wg_stream_t stream);
+/* Device pointers of pair p's output slots (valid until destroy; contents as
+ * of the last run; x/z hold capacity*words words, coeffs 2*capacity doubles;
+ * the first counts[p] terms are the result). */
+int wg_products_batch_result(wg_products_batch_t batch, size_t pair, uint64_t** x, uint64_t** z,
+                             double** coeffs, size_t* capacity);
+/* Device array of n_pairs uint64 term counts, written by every run. */
+int wg_products_batch_counts(wg_products_batch_t batch, uint64_t** counts);
+/* Products and distinct (pair, key) slots of the batch. */
+int wg_products_batch_info(wg_products_batch_t batch, size_t* n_products, size_t* n_keys);
+/* Waits for the device, then frees the batch. */
+int wg_products_batch_destroy(wg_products_batch_t batch);
+
 /* Sort-reduce algorithm behind wg_simplify and the simplifying modes of
  * wg_pauli_products.  No reference counterpart (the reference has one sort);
  * both algorithms give identical results, bit for bit.

@@ -67,6 +67,13 @@ _SIGNATURES: dict[str, list] = {
     "wg_u8_count": [_i, _vp, _sz, _sz, _vp, _vp, ctypes.POINTER(ctypes.c_uint64), _vp],
     "wg_simplify": [_i, _sz, _sz, _vp, _vp, _vp, _d, _d, _pvp, _pvp, _pvp, _psz, _vp],
     "wg_pauli_products": [_i, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _sz, _i, _d, _d, _pvp, _pvp, _pvp, _psz, _vp],
+    "wg_products_batch_create": [_i, _sz, _sz, _pvp, _pvp, _pvp, _psz, _pvp, _pvp, _pvp, _psz, _i, _d, _d, _pvp,
+                                 _vp],
+    "wg_products_batch_run": [_vp, _vp],
+    "wg_products_batch_result": [_vp, _sz, _pvp, _pvp, _pvp, _psz],
+    "wg_products_batch_counts": [_vp, _pvp],
+    "wg_products_batch_info": [_vp, _psz, _psz],
+    "wg_products_batch_destroy": [_vp],
     "wg_set_sort_algorithm": [_i],
     "wg_last_sort_algorithm": [],
     "wg_set_bucket_fine_target": [ctypes.c_uint],

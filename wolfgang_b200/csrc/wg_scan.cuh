@@ -133,4 +133,35 @@ void exclusive_scan(const T* in, T* out, size_t n, T* total, cudaStream_t s) {
   wg::check_launch("launch scan");
 }
 
+// Elements of workspace that exclusive_scan_ws needs for n items: the block
+// sums of every level of the recursion.
+inline size_t scan_workspace(size_t n) {
+  if (n <= static_cast<size_t>(kScanChunk)) return 0;
+  const size_t blocks = (n + kScanChunk - 1) / kScanChunk;
+  return blocks + scan_workspace(blocks);
+}
+
+// exclusive_scan with its block sums in a caller's workspace of
+// scan_workspace(n) elements: no allocation, so a sequence of launches that
+// uses it can be captured in a CUDA graph and replayed.
+template <typename T>
+void exclusive_scan_ws(const T* in, T* out, size_t n, T* total, T* ws, cudaStream_t s) {
+  if (n == 0) {
+    if (total) wg::check_cuda(cudaMemsetAsync(total, 0, sizeof(T), s), "clear scan total");
+    return;
+  }
+  const size_t blocks = (n + kScanChunk - 1) / kScanChunk;
+  if (blocks > 0x7fffffffu) wg::throw_invalid("scan length exceeds the launch grid");
+  if (blocks == 1) {
+    chunk_scan_kernel<T><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, total);
+    wg::check_launch("launch scan");
+    return;
+  }
+  chunk_sum_kernel<T><<<static_cast<unsigned>(blocks), kScanThreads, 0, s>>>(in, n, ws);
+  wg::check_launch("launch scan reduce");
+  exclusive_scan_ws<T>(ws, ws, blocks, nullptr, ws + blocks, s);
+  chunk_scan_kernel<T><<<static_cast<unsigned>(blocks), kScanThreads, 0, s>>>(in, out, n, ws, total);
+  wg::check_launch("launch scan");
+}
+
 }  // namespace wgs
