@@ -52,6 +52,35 @@ int wg_runtime_versions(int* runtime_version, int* driver_version);
 int wg_device_info(int ordinal, char* name, size_t name_cap, int* cc_major,
                    int* cc_minor, size_t* total_mem, int* sm_count);
 
+/* ---------------------------------------------------------- autotuner ---- */
+/* Tile shapes and schedules per shape class (new; no reference counterpart).
+ * Tuned: the commutation kernel and its tile and rows per CTA (algo 0 of
+ * wg_commutation_bits, 1-4 mask words), the bucketed sort's fine-bucket
+ * target (wg_pauli_products / wg_simplify when wg_set_bucket_fine_target is
+ * 0), and the group_commuting chunk length.  A class is (operation, mask
+ * words, ceil log2 of the sizes).  Every candidate gives identical results.
+ *   WG_TUNE_OFF     the measured defaults always;
+ *   WG_TUNE_CACHED  (default) cached choices, the defaults elsewhere: no call
+ *                   measures anything;
+ *   WG_TUNE_SEARCH  the first call of a class with no cached choice times
+ *                   every candidate on its own inputs (CUDA events, best of
+ *                   two runs; it synchronises, so make that call outside
+ *                   stream capture) and caches the fastest.
+ * The cache is process-wide; export/import move it between processes as
+ * text lines "<op> <words> <a> <b> <choice>" (op: commute, bucket, group_qwc,
+ * group_full). */
+#define WG_TUNE_OFF 0
+#define WG_TUNE_CACHED 1
+#define WG_TUNE_SEARCH 2
+int wg_autotune_set_mode(int mode);
+int wg_autotune_get_mode(int* mode);
+/* Writes the cache as text (NUL-terminated) when buf has room;
+ * *needed = bytes required including the NUL.  buf may be NULL. */
+int wg_autotune_export(char* buf, size_t cap, size_t* needed);
+/* Adds the classes of `text` to the cache (existing classes are replaced). */
+int wg_autotune_import(const char* text);
+int wg_autotune_clear(void);
+
 /* ------------------------------------------------------------- memory ---- */
 /* Stream-ordered allocations from the device's memory pool; replace the
  * per-call cudaMalloc/cudaFree of src/cuda/device_pauli_sum.cuh:70-113. */

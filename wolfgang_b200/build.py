@@ -53,7 +53,7 @@ CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall",
 SHARED_LINK = ["-l:libstdc++.so.6", "-Wl,--exclude-libs,ALL"]
 
 CU_SOURCES = ["wg_runtime.cu", "wg_commute.cu", "wg_simplify.cu", "wg_bucket.cu", "wg_expect.cu", "wg_group.cu",
-              "wg_batch.cu"]
+              "wg_batch.cu", "wg_tune.cu"]
 CU_HEADERS = ["wg_common.cuh", "wg_scan.cuh"]
 HOST_SOURCES = ["pauli_sum.cpp", "device.cpp"]
 HOST_HEADERS = ["abi.hpp", "guards.hpp"]

@@ -29,6 +29,9 @@ WG_PRODUCTS_RAW = 0
 WG_PRODUCTS_SIMPLIFY = 1
 WG_PRODUCTS_FUSED = 2
 WG_SORT_AUTO = 0
+WG_TUNE_OFF = 0
+WG_TUNE_CACHED = 1
+WG_TUNE_SEARCH = 2
 WG_SORT_LSD = 1
 WG_SORT_BUCKET = 2
 
@@ -74,6 +77,11 @@ _SIGNATURES: dict[str, list] = {
     "wg_products_batch_counts": [_vp, _pvp],
     "wg_products_batch_info": [_vp, _psz, _psz],
     "wg_products_batch_destroy": [_vp],
+    "wg_autotune_set_mode": [_i],
+    "wg_autotune_get_mode": [ctypes.POINTER(_i)],
+    "wg_autotune_export": [ctypes.c_char_p, _sz, _psz],
+    "wg_autotune_import": [ctypes.c_char_p],
+    "wg_autotune_clear": [],
     "wg_set_sort_algorithm": [_i],
     "wg_last_sort_algorithm": [],
     "wg_set_bucket_fine_target": [ctypes.c_uint],
@@ -175,6 +183,32 @@ _sort_setting = [WG_SORT_AUTO]
 def set_bucket_fine_target(items: int) -> None:
     """Target items per fine bucket of the bucketed sort (0: the default, 896); results do not change."""
     check(lib().wg_set_bucket_fine_target(int(items)))
+
+
+def autotune_mode(mode: int | None = None) -> int:
+    """Returns the autotuner mode (WG_TUNE_*); sets it first when ``mode`` is given."""
+    if mode is not None:
+        check(lib().wg_autotune_set_mode(int(mode)))
+    m = _i(0)
+    check(lib().wg_autotune_get_mode(ctypes.byref(m)))
+    return m.value
+
+
+def autotune_export() -> str:
+    """The autotuner's cache as text, one '<op> <words> <a> <b> <choice>' line per class."""
+    need = ctypes.c_size_t(0)
+    check(lib().wg_autotune_export(None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(need.value + 64)
+    check(lib().wg_autotune_export(buf, len(buf), ctypes.byref(need)))
+    return buf.value.decode()
+
+
+def autotune_import(text: str) -> None:
+    check(lib().wg_autotune_import(text.encode()))
+
+
+def autotune_clear() -> None:
+    check(lib().wg_autotune_clear())
 
 
 def kernel_launches() -> int:

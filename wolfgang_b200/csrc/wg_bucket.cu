@@ -1615,6 +1615,75 @@ __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParam
 
 std::atomic<int> g_sort_algorithm{WG_SORT_AUTO};
 std::atomic<unsigned> g_fine_target{0};  // target items per fine bucket; 0: kFineAvg
+thread_local unsigned t_fine_choice = 0;   // the autotuner's target for the running call; 0: none
+
+// Fine-bucket targets the autotuner chooses among (kFineAvg is candidate 2).
+constexpr unsigned kFineCandidates[] = {640, 768, 896, 1024, 1280};
+static_assert(kFineCandidates[2] == kFineAvg, "the default target is the fallback candidate");
+
+struct FineChoice {
+  explicit FineChoice(unsigned t) { t_fine_choice = t; }
+  ~FineChoice() { t_fine_choice = 0; }
+};
+
+// A bucketed call with the fine-bucket target chosen by the autotuner when
+// no process-wide target is set (wg_set_bucket_fine_target).  call(ox, oz,
+// oc, U) runs the whole sort-reduce and returns false when the bucketed path
+// cannot serve the inputs.  During a search every candidate's run allocates
+// its own outputs; the latest successful run's are kept, the others freed.
+template <class Call>
+bool bucket_tuned(int W, size_t items, uint64_t** ox, uint64_t** oz, double** oc, size_t* U, cudaStream_t s,
+                  Call&& call) {
+  if (g_fine_target.load(std::memory_order_relaxed) != 0) return call(ox, oz, oc, U);
+  uint64_t *kx = nullptr, *kz = nullptr;
+  double* kc = nullptr;
+  size_t ku = 0;
+  bool have = false;
+  auto run = [&](int c) -> bool {
+    FineChoice fc(kFineCandidates[c]);
+    uint64_t *x = nullptr, *z = nullptr;
+    double* cc = nullptr;
+    size_t u = 0;
+    if (!call(&x, &z, &cc, &u)) return false;
+    if (have) {
+      wg::pool_free(kx, s);
+      wg::pool_free(kz, s);
+      wg::pool_free(kc, s);
+    }
+    kx = x;
+    kz = z;
+    kc = cc;
+    ku = u;
+    have = true;
+    return true;
+  };
+  bool done = false;
+  int choice;
+  try {
+    choice = wg::tune_choose(wg::kTuneBucket, W, wg::ceil_log2(items), 0, 2, true, s, run, &done);
+  } catch (...) {
+    if (have) {
+      wg::pool_free(kx, s);
+      wg::pool_free(kz, s);
+      wg::pool_free(kc, s);
+    }
+    throw;
+  }
+  if (done) {
+    *ox = kx;
+    *oz = kz;
+    *oc = kc;
+    *U = ku;
+    return true;
+  }
+  if (have) {  // a search whose candidates all failed but one earlier run
+    wg::pool_free(kx, s);
+    wg::pool_free(kz, s);
+    wg::pool_free(kc, s);
+  }
+  FineChoice fc(kFineCandidates[choice >= 0 && choice < 5 ? choice : 2]);
+  return call(ox, oz, oc, U);
+}
 thread_local int t_last_sort = 0;
 
 struct ThrSpec {
@@ -1673,7 +1742,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   const uint64_t avg = (static_cast<uint64_t>(n) + B1 - 1) / B1;
   const uint64_t capc64 = 2 * avg + 8192;
   const unsigned set_avg = g_fine_target.load(std::memory_order_relaxed);
-  const unsigned favg = set_avg ? set_avg : static_cast<unsigned>(kFineAvg);
+  const unsigned favg = t_fine_choice ? t_fine_choice : set_avg ? set_avg : static_cast<unsigned>(kFineAvg);
   if (capc64 > static_cast<uint64_t>(kFineMax) * favg) return false;  // fine buckets would overflow
   const uint32_t capc = static_cast<uint32_t>(capc64);
   const size_t region = static_cast<size_t>(B1) * capc;
@@ -1856,6 +1925,16 @@ int read_sig(const wg::Scratch& sig, int KW, SigWords& out, cudaStream_t s) {
 
 namespace wg {
 
+// One bucketed sort-reduce with the fine-bucket target of the calling
+// thread's current choice (see bucket_tuned).
+bool bucket_products_once(int device, int W, const uint64_t* lx, const uint64_t* lz, const double* lc, size_t n_l,
+                          const uint64_t* rx, const uint64_t* rz, const double* rc, size_t n_r, int thr_mode,
+                          double atol, double rtol, double thr_fixed, uint64_t** ox, uint64_t** oz, double** oc,
+                          size_t* U, cudaStream_t s);
+bool bucket_simplify_once(int device, int W, const uint64_t* x, const uint64_t* z, const double* c, size_t n,
+                          int thr_mode, double atol, double rtol, uint64_t** ox, uint64_t** oz, double** oc,
+                          size_t* U, cudaStream_t s);
+
 int sort_algorithm() { return g_sort_algorithm.load(std::memory_order_relaxed); }
 void note_sort(int algo) { t_last_sort = algo; }
 
@@ -1866,6 +1945,26 @@ bool bucket_products(int device, int W, const uint64_t* lx, const uint64_t* lz, 
   if (W < 1 || W > 2 || n_l == 0 || n_r == 0 || n_l > 0xffffffffull || n_r > 0xffffffffull) return false;
   const size_t P = n_l * n_r;
   if (P > 0xffffffffull) return false;
+  return bucket_tuned(W, P, ox, oz, oc, U, s, [&](uint64_t** x, uint64_t** z, double** c, size_t* u) {
+    return bucket_products_once(device, W, lx, lz, lc, n_l, rx, rz, rc, n_r, thr_mode, atol, rtol, thr_fixed, x, z,
+                                c, u, s);
+  });
+}
+
+bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, const double* c, size_t n,
+                     int thr_mode, double atol, double rtol, uint64_t** ox, uint64_t** oz, double** oc, size_t* U,
+                     cudaStream_t s) {
+  if (W < 1 || W > 2 || n == 0 || n > 0xffffffffull) return false;
+  return bucket_tuned(W, n, ox, oz, oc, U, s, [&](uint64_t** px, uint64_t** pz, double** pc, size_t* u) {
+    return bucket_simplify_once(device, W, x, z, c, n, thr_mode, atol, rtol, px, pz, pc, u, s);
+  });
+}
+
+bool bucket_products_once(int device, int W, const uint64_t* lx, const uint64_t* lz, const double* lc, size_t n_l,
+                          const uint64_t* rx, const uint64_t* rz, const double* rc, size_t n_r, int thr_mode,
+                          double atol, double rtol, double thr_fixed, uint64_t** ox, uint64_t** oz, double** oc,
+                          size_t* U, cudaStream_t s) {
+  const size_t P = n_l * n_r;
   const int KW = 2 * W;
   Scratch sig(sizeof(unsigned long long) * 4, s);
   check_cuda(cudaMemsetAsync(sig.get(), 0, sizeof(unsigned long long) * 4, s), "clear significant bits");
@@ -1888,10 +1987,9 @@ bool bucket_products(int device, int W, const uint64_t* lx, const uint64_t* lz, 
   return run_bucket<4>(device, src, static_cast<uint32_t>(P), total, thr, out, s);
 }
 
-bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, const double* c, size_t n,
-                     int thr_mode, double atol, double rtol, uint64_t** ox, uint64_t** oz, double** oc, size_t* U,
-                     cudaStream_t s) {
-  if (W < 1 || W > 2 || n == 0 || n > 0xffffffffull) return false;
+bool bucket_simplify_once(int device, int W, const uint64_t* x, const uint64_t* z, const double* c, size_t n,
+                          int thr_mode, double atol, double rtol, uint64_t** ox, uint64_t** oz, double** oc,
+                          size_t* U, cudaStream_t s) {
   const int KW = 2 * W;
   Scratch sig(sizeof(unsigned long long) * 4, s);
   check_cuda(cudaMemsetAsync(sig.get(), 0, sizeof(unsigned long long) * 4, s), "clear significant bits");

@@ -13,6 +13,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "wg_pauli.h"
 
@@ -222,6 +223,65 @@ bool bucket_simplify(int device, int W, const uint64_t* x, const uint64_t* z, co
                      cudaStream_t s);
 int sort_algorithm();     // WG_SORT_* setting
 void note_sort(int algo);  // records the algorithm of the thread's last result
+
+// ------------------------------------------------------------- autotuner
+// Tile shapes and schedules chosen per shape class (wg_tune.cu).  A class is
+// (operation, mask words, a, b) with a and b the ceiling log2 of the sizes
+// that set the work (e.g. lhs and rhs terms).  In WG_TUNE_SEARCH mode the
+// first call of a class without a cached choice runs every candidate on its
+// own inputs, times each on its stream with CUDA events (best of two runs),
+// synchronising, and caches the fastest; WG_TUNE_CACHED (default) uses cached
+// choices and the measured defaults elsewhere; WG_TUNE_OFF always the
+// defaults.  Every candidate of an operation produces identical results.
+enum TuneOp : int { kTuneCommute = 1, kTuneBucket = 2, kTuneGroupQwc = 3, kTuneGroupFull = 4 };
+int tune_mode();
+int tune_lookup(int op, int words, int a, int b);  // -1 when the class has no cached choice
+void tune_store(int op, int words, int a, int b, int choice);
+int tune_candidates(int op);  // number of candidates of an operation
+int ceil_log2(size_t n);
+// Milliseconds of run() on stream s (CUDA events; synchronises s); run()
+// returns false when its candidate cannot serve the inputs (infinite time).
+float tune_time(cudaStream_t s, bool (*run)(void*), void* ctx);
+
+// The choice for one call: the class's cached choice, else (search mode, and
+// allow_search) the fastest candidate, else `fallback`.  run(c) does the
+// call's whole work with candidate c and returns false if c cannot serve it;
+// after a search the last candidate's run has produced the call's results
+// (all candidates' results are identical), and *done says so.
+template <class Run>
+int tune_choose(int op, int words, int a, int b, int fallback, bool allow_search, cudaStream_t s, Run&& run,
+                bool* done) {
+  *done = false;
+  const int mode = tune_mode();
+  if (mode == WG_TUNE_OFF) return fallback;
+  const int cached = tune_lookup(op, words, a, b);
+  if (cached >= 0) return cached;
+  if (mode != WG_TUNE_SEARCH || !allow_search) return fallback;
+  const int n = tune_candidates(op);
+  int best = -1;
+  float best_ms = 0.0f;
+  for (int c = 0; c < n; ++c) {
+    struct Ctx {
+      std::remove_reference_t<Run>* run;
+      int c;
+    } ctx{&run, c};
+    auto thunk = [](void* p) -> bool {
+      auto* k = static_cast<Ctx*>(p);
+      return (*k->run)(k->c);
+    };
+    float ms = tune_time(s, thunk, &ctx);
+    const float ms2 = tune_time(s, thunk, &ctx);  // the first run may carry one-time set-up
+    if (ms2 < ms) ms = ms2;
+    if (ms >= 0.0f && (best < 0 || ms < best_ms)) {
+      best = c;
+      best_ms = ms;
+    }
+  }
+  if (best < 0) return fallback;
+  *done = true;  // the last successful run left the results in place
+  tune_store(op, words, a, b, best);
+  return best;
+}
 
 inline size_t checked_mul(size_t a, size_t b, const char* what) {
   if (a != 0 && b > SIZE_MAX / a) throw_invalid(std::string(what) + " size overflows size_t");

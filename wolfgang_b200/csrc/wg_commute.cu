@@ -306,7 +306,7 @@ void launch_ballot(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uin
 
 template <int W, int LW, int THREADS>
 void launch_plane_as(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx, const uint64_t* rz,
-                     size_t n_r, uint32_t* bits, size_t pitch, int device, cudaStream_t s) {
+                     size_t n_r, uint32_t* bits, size_t pitch, int device, cudaStream_t s, size_t max_rows = 16384) {
   constexpr int kWordsCta = 32 * LW;
   auto* kernel = commute_plane_kernel<W, LW, THREADS>;
   const size_t smem = static_cast<size_t>(64 * W) * 2 * kWordsCta * sizeof(uint32_t);
@@ -324,7 +324,7 @@ void launch_plane_as(const uint64_t* lx, const uint64_t* lz, size_t n_l, const u
   // terms 2,048 rows per CTA took 5.93 ms, 4,096 4.57, 8,192 3.88, 16,384 3.52
   // (32,768 rows at two CTAs per SM 3.80: the last wave runs part empty).
   const size_t sms = wg::device_props(device).sm_count;
-  size_t rows_per_cta = 16384;
+  size_t rows_per_cta = max_rows;
   while (rows_per_cta > 256 && col_blocks * ((n_l + rows_per_cta - 1) / rows_per_cta) < 4 * sms)
     rows_per_cta /= 2;
   size_t row_chunks = (n_l + rows_per_cta - 1) / rows_per_cta;
@@ -338,22 +338,52 @@ void launch_plane_as(const uint64_t* lx, const uint64_t* lz, size_t n_l, const u
   wg::check_launch("launch commutation (bit-plane)");
 }
 
-// Four output words per lane and 1,024 threads (4,096-column tiles) for one or
-// two mask words when both sides are large: measured 5.9 against 7.2 ms on
-// 262,144^2 terms.  Smaller products keep two words per lane and 256 threads,
-// where the wider tile's plane building would not be amortised over enough
-// rows (32,768^2 terms: 433 against 253 us).
+// Candidates of the commutation autotuner (wg_tune.cu) on 1-4 mask words:
+//   0 ballot kernel;
+//   1 bit-plane, two output words per lane, 256 threads (2,048-column tiles);
+//   2 bit-plane, four output words per lane, 1,024 threads (4,096-column
+//     tiles; 1-2 mask words only: the planes of 4,096 columns take 64 KB of
+//     shared memory per mask word and side);
+//   3, 4 as 1, 2 with at most 2,048 lhs rows per CTA (more CTAs, each
+//     building its plane tile for fewer rows).
+// Returns false when the candidate does not serve this width.
 template <int W>
-void launch_plane(const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
-                  const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, int device,
-                  cudaStream_t s) {
-  if constexpr (W <= 2) {
-    if (n_l >= 65536 && n_r >= 65536) {
-      launch_plane_as<W, 4, 1024>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
-      return;
-    }
+bool launch_candidate_w(int c, const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
+                        const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, int device, cudaStream_t s) {
+  switch (c) {
+    case 0: launch_ballot<W>(lx, lz, n_l, rx, rz, n_r, bits, pitch, s); return true;
+    case 1: launch_plane_as<W, 2, 256>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s); return true;
+    case 3: launch_plane_as<W, 2, 256>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s, 2048); return true;
+    case 2:
+    case 4:
+      if constexpr (W <= 2) {
+        launch_plane_as<W, 4, 1024>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s, c == 2 ? 16384 : 2048);
+        return true;
+      }
+      return false;
+    default: return false;
   }
-  launch_plane_as<W, 2, 256>(lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
+}
+
+bool launch_candidate(int c, size_t words, const uint64_t* lx, const uint64_t* lz, size_t n_l, const uint64_t* rx,
+                      const uint64_t* rz, size_t n_r, uint32_t* bits, size_t pitch, int device, cudaStream_t s) {
+  switch (words) {
+    case 1: return launch_candidate_w<1>(c, lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
+    case 2: return launch_candidate_w<2>(c, lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
+    case 3: return launch_candidate_w<3>(c, lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
+    case 4: return launch_candidate_w<4>(c, lx, lz, n_l, rx, rz, n_r, bits, pitch, device, s);
+    default: return false;
+  }
+}
+
+// The measured default tile for the bit-plane kernel: four output words per
+// lane and 1,024 threads (4,096-column tiles) for one or two mask words when
+// both sides are large: 5.9 against 7.2 ms on 262,144^2 terms.  Smaller
+// products keep two words per lane and 256 threads, where the wider tile's
+// plane building would not be amortised over enough rows (32,768^2 terms: 433
+// against 253 us).
+int default_plane_candidate(size_t W, size_t n_l, size_t n_r) {
+  return (W <= 2 && n_l >= 65536 && n_r >= 65536) ? 2 : 1;
 }
 
 // Default choice between the two algorithms, from the sizes and the word
@@ -375,14 +405,11 @@ int default_algo(size_t W, size_t n_l, size_t n_r) {
   return 2;
 }
 
-}  // namespace
-
-extern "C" {
-
-int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x, const uint64_t* lhs_z,
-                        size_t n_lhs, const uint64_t* rhs_x, const uint64_t* rhs_z, size_t n_rhs,
-                        uint32_t* bits, size_t pitch_words, int algo, wg_stream_t stream) {
-  return wg::guarded([&] {
+// wg_commutation_bits' work.  allow_search = false never measures (the
+// no-allocation entry point): cached autotuner choices or the defaults only.
+void commutation_bits(int device, size_t words, const uint64_t* lhs_x, const uint64_t* lhs_z, size_t n_lhs,
+                      const uint64_t* rhs_x, const uint64_t* rhs_z, size_t n_rhs, uint32_t* bits,
+                      size_t pitch_words, int algo, bool allow_search, cudaStream_t stream) {
     if (pitch_words < (n_rhs + 31) / 32) wg::throw_invalid("commutation bit matrix pitch is too small");
     if (algo < 0 || algo > 2) wg::throw_invalid("commutation algo must be 0, 1 or 2");
     if (n_lhs == 0 || n_rhs == 0) return;
@@ -395,28 +422,42 @@ int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x, const u
       wg::check_launch("launch commutation fill");
       return;
     }
-    if (algo == 0) algo = default_algo(words, n_lhs, n_rhs);
-    if (algo == 2 && words <= 4) {
-      switch (words) {
-        case 1: launch_plane<1>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
-        case 2: launch_plane<2>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
-        case 3: launch_plane<3>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
-        case 4: launch_plane<4>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s); return;
-      }
+    if (words <= 4) {
+      const int plane = default_plane_candidate(words, n_lhs, n_rhs);
+      const int fallback = algo == 1 ? 0 : algo == 2 ? plane : (default_algo(words, n_lhs, n_rhs) == 1 ? 0 : plane);
+      int choice = fallback;
+      bool done = false;
+      if (algo == 0)
+        choice = wg::tune_choose(
+            wg::kTuneCommute, static_cast<int>(words), wg::ceil_log2(n_lhs), wg::ceil_log2(n_rhs), fallback,
+            allow_search, s,
+            [&](int c) {
+              return launch_candidate(c, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device,
+                                      s);
+            },
+            &done);
+      if (!done && !launch_candidate(choice, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words,
+                                     device, s))
+        launch_candidate(fallback, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, device, s);
+      return;
     }
-    switch (words) {
-      case 1: launch_ballot<1>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
-      case 2: launch_ballot<2>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
-      case 3: launch_ballot<3>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
-      case 4: launch_ballot<4>(lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, s); return;
-      default: {
-        const size_t items = n_lhs * ((n_rhs + 31) / 32);
-        WG_TIMED("commute_generic_kernel", s,
-          commute_generic_kernel<<<wg::grid_for(items * 32, 256, device, 8), 256, 0, s>>>(
-              lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, words, bits, pitch_words));
-        wg::check_launch("launch commutation (generic)");
-      }
-    }
+    const size_t items = n_lhs * ((n_rhs + 31) / 32);
+    WG_TIMED("commute_generic_kernel", s,
+      commute_generic_kernel<<<wg::grid_for(items * 32, 256, device, 8), 256, 0, s>>>(
+          lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, words, bits, pitch_words));
+    wg::check_launch("launch commutation (generic)");
+}
+
+}  // namespace
+
+extern "C" {
+
+int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x, const uint64_t* lhs_z,
+                        size_t n_lhs, const uint64_t* rhs_x, const uint64_t* rhs_z, size_t n_rhs,
+                        uint32_t* bits, size_t pitch_words, int algo, wg_stream_t stream) {
+  return wg::guarded([&] {
+    commutation_bits(device, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch_words, algo, true,
+                     stream);
   });
 }
 
@@ -636,10 +677,12 @@ extern "C" int wg_commutation_u8_noalloc(int device, size_t words, const uint64_
                         std::to_string(bytes) + " bytes exceeds the 32 MiB static scratch");
     wg::DeviceGuard g(device);
     uint32_t* bits = noalloc_scratch(device);
-    // The existing entry points do the work; they allocate nothing themselves.
-    int rc = wg_commutation_bits(device, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch, 0, stream);
-    if (rc != WG_OK) throw wg::Error(rc, wg_last_error());
-    rc = wg_bits_to_u8(device, bits, n_lhs, n_rhs, pitch, out, stream);
+    // The ordinary path's kernels do the work; they allocate nothing
+    // themselves.  The kernel choice reads no term data and never measures
+    // (the autotuner's cached choice or the size rule), so a call after the
+    // first synchronises nothing.
+    commutation_bits(device, words, lhs_x, lhs_z, n_lhs, rhs_x, rhs_z, n_rhs, bits, pitch, 0, false, stream);
+    const int rc = wg_bits_to_u8(device, bits, n_lhs, n_rhs, pitch, out, stream);
     if (rc != WG_OK) throw wg::Error(rc, wg_last_error());
   });
   return status;

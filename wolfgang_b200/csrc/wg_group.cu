@@ -452,10 +452,16 @@ __global__ void group_out_kernel(const uint32_t* __restrict__ order, const uint3
   }
 }
 
+// Chunk lengths the autotuner chooses among (the measured defaults above are
+// candidates 2 and 1); every chunk length gives the same groups.
+constexpr uint32_t kQwcChunks[] = {256, 512, 1024};
+constexpr uint32_t kFullChunks[] = {64, 96, 128, 192};
+static_assert(kQwcChunks[2] == kChunk && kFullChunks[1] == kChunkFull, "defaults are candidates");
+
 template <int W>
 void run_greedy(int device, bool full, const uint64_t* ox, const uint64_t* oz, uint32_t T, uint64_t* rows,
                 uint32_t* first, uint32_t* last, uint32_t* next, uint32_t* lb, uint32_t* lbm, uint32_t* gid,
-                uint32_t* ng, cudaStream_t s) {
+                uint32_t* ng, cudaStream_t s, uint32_t chunk) {
   const auto& props = wg::device_props(device);
   auto* kb = full ? group_bound_kernel<W, true> : group_bound_kernel<W, false>;
   auto* kr = full ? group_resolve_kernel<W, true> : group_resolve_kernel<W, false>;
@@ -471,7 +477,7 @@ void run_greedy(int device, bool full, const uint64_t* ox, const uint64_t* oz, u
                  "set group resolve shared memory");
   wg::check_cuda(cudaMemsetAsync(ng, 0, 4, s), "clear group count");
   const unsigned max_blocks = static_cast<unsigned>(props.sm_count) * 8;
-  const uint32_t chunk = full ? kChunkFull : kChunk;
+  if (chunk == 0 || chunk > static_cast<uint32_t>(kChunk)) chunk = full ? kChunkFull : kChunk;  // staging holds kChunk
   for (uint32_t c0 = 0; c0 < T; c0 += chunk) {
     const uint32_t c1 = T - c0 > chunk ? c0 + chunk : T;
     const unsigned blocks = std::min<unsigned>(max_blocks, (c1 - c0 + kBoundThreads / 32 - 1) / (kBoundThreads / 32));
@@ -858,27 +864,40 @@ int wg_group_commuting(int device, size_t words, size_t n_terms, const uint64_t*
             ox.as<uint64_t>(), oz.as<uint64_t>(), T, W, trows.as<uint64_t>()));
       wg::check_launch("launch interleave rows");
     }
-    switch (W) {
-      case 0:
-      case 1: run_greedy<1>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
-                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
-                               ng.as<uint32_t>(), s); break;
-      case 2: run_greedy<2>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
-                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
-                               ng.as<uint32_t>(), s); break;
-      case 3: run_greedy<3>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
-                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
-                               ng.as<uint32_t>(), s); break;
-      case 4: run_greedy<4>(device, full, ox.as<uint64_t>(), oz.as<uint64_t>(), T32, rows.as<uint64_t>(),
-                               first.as<uint32_t>(), last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(),
-                               lbm.as<uint32_t>(), gid.as<uint32_t>(),
-                               ng.as<uint32_t>(), s); break;
-      default: run_greedy_n(device, full, W, trows.as<uint64_t>(), T32, rows.as<uint64_t>(), first.as<uint32_t>(),
-                            last.as<uint32_t>(), next.as<uint32_t>(), lb.as<uint32_t>(), lbm.as<uint32_t>(),
-                            gid.as<uint32_t>(), ng.as<uint32_t>(), s); break;
+    auto greedy = [&](uint32_t chunk) {
+      auto* r = rows.as<uint64_t>();
+      auto* f = first.as<uint32_t>();
+      auto* l = last.as<uint32_t>();
+      auto* nx = next.as<uint32_t>();
+      auto* b = lb.as<uint32_t>();
+      auto* bm = lbm.as<uint32_t>();
+      auto* gi = gid.as<uint32_t>();
+      auto* n = ng.as<uint32_t>();
+      const uint64_t* px = ox.as<uint64_t>();
+      const uint64_t* pz = oz.as<uint64_t>();
+      switch (W) {
+        case 0:
+        case 1: run_greedy<1>(device, full, px, pz, T32, r, f, l, nx, b, bm, gi, n, s, chunk); break;
+        case 2: run_greedy<2>(device, full, px, pz, T32, r, f, l, nx, b, bm, gi, n, s, chunk); break;
+        case 3: run_greedy<3>(device, full, px, pz, T32, r, f, l, nx, b, bm, gi, n, s, chunk); break;
+        case 4: run_greedy<4>(device, full, px, pz, T32, r, f, l, nx, b, bm, gi, n, s, chunk); break;
+        default: run_greedy_n(device, full, W, trows.as<uint64_t>(), T32, r, f, l, nx, b, bm, gi, n, s); break;
+      }
+    };
+    if (W <= 4) {
+      // chunk length: the autotuner's choice for (mode, words, log2 terms)
+      const uint32_t* cands = full ? kFullChunks : kQwcChunks;
+      bool done = false;
+      const int choice = wg::tune_choose(
+          full ? wg::kTuneGroupFull : wg::kTuneGroupQwc, W, wg::ceil_log2(T), 0, full ? 1 : 2, true, s,
+          [&](int c) {
+            greedy(cands[c]);
+            return true;
+          },
+          &done);
+      if (!done) greedy(cands[choice]);
+    } else {
+      greedy(0);
     }
     uint32_t G = 0;
     wg::check_cuda(cudaMemcpyAsync(&G, ng.get(), 4, cudaMemcpyDeviceToHost, s), "read group count");
