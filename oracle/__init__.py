@@ -201,6 +201,18 @@ class Oracle:
                                      _p(_ptr(psi)), _p(_ptr(out))))
         return out
 
+    def hpsi_at(self, n, x, z, c, psi, idx) -> np.ndarray:
+        """(H psi)[idx] (complex128), the or_hpsi sum at the listed amplitudes only."""
+        T = len(c)
+        w = words_for(n)
+        x, z, c = _u64(x, T, w), _u64(z, T, w), _c128(c, T)
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        idx = np.ascontiguousarray(np.asarray(idx, np.uint64))
+        out = np.zeros(len(idx), np.complex128)
+        self._check(self.lib.or_hpsi_at(_sz(T), _sz(n), _p(_ptr(x)), _p(_ptr(z)), _p(_ptr(c)), _p(_ptr(psi)),
+                                        _sz(len(idx)), _p(_ptr(idx)), _p(_ptr(out))))
+        return out
+
     def expectation_z_counts(self, n, x, z, c, packed, counts) -> complex:
         T = len(c)
         w = words_for(n)

@@ -260,21 +260,44 @@ int or_matmul_keyrange(size_t nl, size_t nr, size_t words, const uint64_t* lx,
   std::vector<uint64_t> sx, sz;
   std::vector<cplx> sc;
   std::vector<uint64_t> px(w), pz(w);
+  // The threshold atol + 0 * max|product| (src/simplify.cpp:156-160) is atol
+  // unless some product's magnitude is infinite (0 * inf = NaN culls all).
+  // When every input coefficient is finite and max|a| * max|b| is far below
+  // the overflow limit, no product can be infinite, and the magnitudes of the
+  // products outside the range need not be formed; otherwise every product's
+  // magnitude enters the maximum, as in or_matmul.
+  double amax = 0.0, bmax = 0.0;
+  bool finite = true;
+  for (size_t a = 0; a < nl; ++a) {
+    const cplx v = load_c(lc, a);
+    finite = finite && std::isfinite(v.real()) && std::isfinite(v.imag());
+    amax = std::max(amax, std::abs(v));
+  }
+  for (size_t b = 0; b < nr; ++b) {
+    const cplx v = load_c(rc, b);
+    finite = finite && std::isfinite(v.real()) && std::isfinite(v.imag());
+    bmax = std::max(bmax, std::abs(v));
+  }
+  const bool need_max = !fused_threshold && !(finite && amax < 1e150 && bmax < 1e150);
   double max_abs = 0.0;
   for (size_t a = 0; a < nl; ++a) {
     const cplx ca = load_c(lc, a);
     for (size_t b = 0; b < nr; ++b) {
-      int64_t e = -ly[a] - ry[b];
       for (size_t k = 0; k < w; ++k) {
         px[k] = lx[a * w + k] ^ rx[b * w + k];
         pz[k] = lz[a * w + k] ^ rz[b * w + k];
+      }
+      const bool in_range = compare_keys(px.data(), pz.data(), klo_x.data(), klo_z.data(), w) >= 0 &&
+                            compare_keys(px.data(), pz.data(), khi_x.data(), khi_z.data(), w) < 0;
+      if (!in_range && !need_max) continue;
+      int64_t e = -ly[a] - ry[b];
+      for (size_t k = 0; k < w; ++k) {
         e += std::popcount(px[k] & pz[k]);
         e += 2 * static_cast<int64_t>(std::popcount(lx[a * w + k] & rz[b * w + k]));
       }
       const cplx v = rotate(ca * load_c(rc, b), e);
-      if (!fused_threshold) max_abs = std::max(max_abs, std::abs(v));
-      if (compare_keys(px.data(), pz.data(), klo_x.data(), klo_z.data(), w) < 0) continue;
-      if (compare_keys(px.data(), pz.data(), khi_x.data(), khi_z.data(), w) >= 0) continue;
+      if (need_max) max_abs = std::max(max_abs, std::abs(v));
+      if (!in_range) continue;
       sx.insert(sx.end(), px.begin(), px.end());
       sz.insert(sz.end(), pz.begin(), pz.end());
       sc.push_back(v);
@@ -282,8 +305,17 @@ int or_matmul_keyrange(size_t nl, size_t nr, size_t words, const uint64_t* lx,
   }
   const double thr = fused_threshold ? 1.0e-12 : 1.0e-12 + 0.0 * max_abs;
   const size_t S = sc.size();
-  if (S > cap) return fail("or_matmul_keyrange capacity too small");
-  reduce_sorted(S, w, sx.data(), sz.data(), sc.data(), thr, ox, oz, oc, out_terms);
+  // reduce into scratch sized for every in-range product, then hand over the
+  // survivors: cap only bounds the result
+  std::vector<uint64_t> tx(S * w + 1), tz(S * w + 1);
+  std::vector<double> tc(2 * S + 2);
+  size_t u = 0;
+  reduce_sorted(S, w, sx.data(), sz.data(), sc.data(), thr, tx.data(), tz.data(), tc.data(), &u);
+  if (u > cap) return fail("or_matmul_keyrange capacity too small");
+  std::copy(tx.begin(), tx.begin() + static_cast<std::ptrdiff_t>(u * w), ox);
+  std::copy(tz.begin(), tz.begin() + static_cast<std::ptrdiff_t>(u * w), oz);
+  std::copy(tc.begin(), tc.begin() + static_cast<std::ptrdiff_t>(2 * u), oc);
+  *out_terms = u;
   return 0;
 }
 
@@ -554,6 +586,36 @@ int or_hpsi(size_t T, size_t n_qubits, const uint64_t* x, const uint64_t* z,
   for (size_t j = 0; j < N; ++j) {
     out[2 * j] = re[j].value();
     out[2 * j + 1] = im[j].value();
+  }
+  return 0;
+}
+
+int or_hpsi_at(size_t T, size_t n_qubits, const uint64_t* x, const uint64_t* z,
+               const double* c, const double* psi, size_t m, const uint64_t* idx,
+               double* out) {
+  // or_hpsi's sum, term by term in the same order, evaluated at the m
+  // requested amplitudes only.
+  if (n_qubits > 63) return fail("expectation_statevector requires num_qubits <= 63");
+  const size_t words = n_qubits == 0 ? 0 : 1;
+  const size_t N = size_t{1} << n_qubits;
+  for (size_t i = 0; i < m; ++i)
+    if (idx[i] >= N) return fail("or_hpsi_at index is out of range");
+  std::vector<KSum> re(m), im(m);
+  for (size_t t = 0; t < T; ++t) {
+    const uint64_t xm = words == 0 ? 0 : x[t * words];
+    const uint64_t zm = words == 0 ? 0 : z[t * words];
+    const cplx d = rotate(load_c(c, t), std::popcount(xm & zm));
+    for (size_t i = 0; i < m; ++i) {
+      const size_t src = static_cast<size_t>(idx[i]) ^ static_cast<size_t>(xm);
+      const cplx v = d * load_c(psi, src);
+      const bool neg = std::popcount(zm & static_cast<uint64_t>(src)) & 1U;
+      re[i].add(neg ? -v.real() : v.real());
+      im[i].add(neg ? -v.imag() : v.imag());
+    }
+  }
+  for (size_t i = 0; i < m; ++i) {
+    out[2 * i] = re[i].value();
+    out[2 * i + 1] = im[i].value();
   }
   return 0;
 }

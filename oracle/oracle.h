@@ -45,7 +45,8 @@ int or_matmul(size_t nl, size_t nr, size_t words, const uint64_t* lx,
  * key_lo <= k < key_hi (keys given as 2*words words in canonical significance
  * order x0,z0,x1,z1,...).  Same summation order and cull as or_matmul, so the
  * result equals the matching slice of or_matmul's output.  Used to check the
- * full-size product workload one key range at a time.  cap = output capacity. */
+ * full-size product workload one key range at a time.  cap = output capacity
+ * (terms); a range with more survivors fails. */
 int or_matmul_keyrange(size_t nl, size_t nr, size_t words, const uint64_t* lx,
                        const uint64_t* lz, const double* lc, const uint64_t* rx,
                        const uint64_t* rz, const double* rc,
@@ -91,6 +92,12 @@ int or_term_expectations(size_t T, size_t n_qubits, const uint64_t* x,
  * src/expectation.cpp:121-150).  psi and out are complex128. */
 int or_hpsi(size_t T, size_t n_qubits, const uint64_t* x, const uint64_t* z,
             const double* c, const double* psi, double* out);
+
+/* (H|psi>)[idx[i]] for i < m: or_hpsi at the listed amplitudes only (for
+ * statevectors whose full H|psi> the oracle cannot afford). */
+int or_hpsi_at(size_t T, size_t n_qubits, const uint64_t* x, const uint64_t* z,
+               const double* c, const double* psi, size_t m, const uint64_t* idx,
+               double* out);
 
 /* PauliSum::expectation_z_counts (src/expectation.cpp:219-247) with bitstrings
  * already packed (row-major, `words` words per row). */

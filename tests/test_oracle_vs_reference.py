@@ -172,3 +172,50 @@ def test_z_counts_errors_match_reference(oracle, reference):
             oracle.expectation_z_counts(n, xx, z, c, packed, counts)
         with pytest.raises(OracleError, match=msg):
             reference.expectation_z_counts(n, xx, z, c, packed, counts)
+
+
+@pytest.mark.parametrize("n,nl,nr,pool,special", [(12, 120, 90, None, None), (70, 200, 150, 40, None),
+                                                 (20, 60, 50, None, "inf"), (20, 60, 50, None, "nan"),
+                                                 (10, 80, 70, None, "huge")])
+def test_matmul_keyranges_tile_the_full_product(oracle, reference, n, nl, nr, pool, special):
+    """or_matmul_keyrange over consecutive key ranges (cut at keys of the full
+    result, plus an empty range before it and one after it) reproduces the
+    reference's matmul + simplify, bit for bit; this is how the full-size
+    product workload is checked range by range.  Non-finite and huge
+    coefficients take the oracle's path that forms every product's magnitude."""
+    rng = np.random.default_rng(zlib.crc32(repr((n, nl, nr, special)).encode()))
+    A = random_operator(rng, n, nl, 0.2, pool)
+    B = random_operator(rng, n, nr, 0.2, pool)
+    if special == "inf":
+        A[3][3] = complex(np.inf, 0.5)
+    elif special == "nan":
+        B[3][5] = complex(np.nan, 1.0)
+    elif special == "huge":
+        A[3][:] *= 1e200
+        B[3][:] *= 1e200
+    raw = reference.matmul(n, A[1:], B[1:], simplify=False)
+    want = reference.simplify(n, *raw, 1e-12, 0.0)
+    w = (n + 63) // 64
+    U = len(want[2])
+
+    def key(i):
+        k = np.zeros(2 * w, np.uint64)
+        k[0::2], k[1::2] = want[0][i], want[1][i]
+        return k
+
+    lo_all = np.zeros(2 * w, np.uint64)
+    hi_all = np.full(2 * w, np.iinfo(np.uint64).max, np.uint64)
+    cuts = [lo_all] + [key(i) for i in range(0, U, max(1, U // 5))] + [hi_all]
+    got = [oracle.matmul_keyrange(n, A[1:], B[1:], lo, hi, cap=nl * nr) for lo, hi in zip(cuts[:-1], cuts[1:])]
+    for k in range(3):
+        assert same_bits(np.concatenate([g[k] for g in got]), want[k])
+
+
+def test_hpsi_at_equals_full_hpsi(oracle):
+    """or_hpsi_at (H psi at listed amplitudes) is the full or_hpsi, element for element."""
+    rng = np.random.default_rng(8)
+    n, x, z, c = random_operator(rng, 11, 90, 0.3)
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    full = oracle.hpsi(n, x, z, c, psi)
+    idx = rng.integers(0, 1 << n, size=200, dtype=np.uint64)
+    assert same_bits(oracle.hpsi_at(n, x, z, c, psi, idx), full[idx.astype(np.int64)])
