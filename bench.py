@@ -272,6 +272,59 @@ def reference_products_sample(A, B, rows: int) -> tuple[float, int]:
     return time.perf_counter() - t0, rows * len(bc)
 
 
+def products_parity(torch, L, A, B, W, ax, az, ac, bx, bz, bc, sh, span: int = 1 << 20) -> dict:
+    """One more device call of the products workload, checked against the
+    oracle on the key ranges of its first and last `span` survivors: those
+    survivors must equal the oracle's matmul + simplify over the same ranges
+    bit for bit (keys, order, coefficient bits)."""
+    import ctypes as ct
+
+    from oracle import Oracle
+    from wolfgang_b200 import capi
+
+    nl, nr = len(A[3]), len(B[3])
+    dv = torch.cuda.current_device()
+    ox, oz, oc, Uc = ct.c_void_p(), ct.c_void_p(), ct.c_void_p(), ct.c_size_t()
+    capi.check(L.wg_pauli_products(dv, W, ax.data_ptr(), az.data_ptr(), ac.data_ptr(), nl, bx.data_ptr(),
+                                   bz.data_ptr(), bc.data_ptr(), nr, capi.WG_PRODUCTS_SIMPLIFY, 1e-12, 0.0,
+                                   ct.byref(ox), ct.byref(oz), ct.byref(oc), ct.byref(Uc), sh))
+    U = Uc.value
+
+    def fetch(p0, p1):
+        x = np.empty((p1 - p0, W), np.uint64)
+        z = np.empty((p1 - p0, W), np.uint64)
+        c = np.empty(p1 - p0, np.complex128)
+        for arr, ptr, size in ((x, ox, 8 * W), (z, oz, 8 * W), (c, oc, 16)):
+            capi.check(L.wg_memcpy_dtoh(dv, arr.ctypes.data, ptr.value + p0 * size, arr.nbytes, sh))
+        return x, z, c
+
+    def key(x, z, i):
+        k = np.zeros(2 * W, np.uint64)
+        k[0::2], k[1::2] = x[i], z[i]
+        return k
+
+    orc = Oracle()
+    checked, exact, worst = 0, True, 0.0
+    t0 = time.perf_counter()
+    for p0 in (0, max(0, U - span - 1)):
+        p1 = min(U, p0 + span + 1)
+        x, z, c = fetch(p0, p1)
+        lo, hi = key(x, z, 0), key(x, z, len(c) - 1)  # [first, last): the range's last survivor bounds it
+        want = orc.matmul_keyrange(A[0], A[1:], B[1:], lo, hi, cap=len(c))
+        got = (x[:-1], z[:-1], c[:-1])
+        exact = exact and all(np.ascontiguousarray(g).tobytes() == np.ascontiguousarray(w).tobytes()
+                              for g, w in zip(got, want))
+        if len(want[2]) == len(got[2]):
+            worst = max(worst, float(np.max(np.abs(got[2] - want[2]))) if len(got[2]) else 0.0)
+        checked += len(got[2])
+    for q in (ox, oz, oc):
+        capi.check(L.wg_free(dv, q, sh))
+    return {"survivors_checked": checked, "survivors": U, "bit_exact": bool(exact), "max_abs_err": worst,
+            "how": f"oracle matmul+simplify over the key ranges of the first and last {span} survivors "
+                   f"({time.perf_counter() - t0:.1f} s); the whole result is checked range by range by "
+                   "tests/test_gpu_fullsize.py"}
+
+
 def bench_products(args, world, rank, torch) -> dict:
     from wolfgang_b200 import capi
     from wolfgang_b200.workloads import klocal_pair_100q
@@ -425,6 +478,7 @@ def bench_products(args, world, rank, torch) -> dict:
                                   f"{avail / 1e9:.0f} GB of free host memory at once: the ranks made their calls "
                                   "one after another; value = all ranks' products / the slowest rank's call")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["parity"] = products_parity(torch, L, A, B, W, ax, az, ac, bx, bz, bc, sh)
         secs, prods = reference_products_sample(A, B, args.cpu_rows)
         out["cpu_baseline"] = {"value": prods / secs, "unit": "terms/s", "cores": 1, "kind": "reference",
                                "extrapolated": True, **host_cpu(),
@@ -503,6 +557,13 @@ def bench_commutation(args, world, rank, torch) -> dict:
         t0 = time.perf_counter()
         ref.commutes(n, (x[:rows], z[:rows]), (x, z))
         dt = time.perf_counter() - t0
+        got = np.unpackbits(bits.view(T, pitch)[:rows].cpu().numpy().view(np.uint8).reshape(rows, -1), axis=1,
+                            bitorder="little")[:, :T]
+        from oracle import Oracle
+
+        want = Oracle().commutes(n, (x[:rows], z[:rows]), (x, z))
+        out["parity"] = {"rows_checked": rows, "pairs_checked": rows * T, "bit_exact": bool(np.array_equal(got, want)),
+                         "how": "the first rows of the device bit matrix against the oracle's flags"}
         out["cpu_baseline"] = {"value": rows * T / dt, "unit": "pairs/s", "cores": 1, "kind": "reference",
                                "extrapolated": True, **host_cpu(), "sample": f"{rows} rows x {T} terms via reference PauliSum::commutes_with "
                                          f"(auto CPU dispatch: {ref.cpu_backend()}), {dt:.1f} s"}
@@ -545,6 +606,17 @@ def bench_grouping(args, world, rank, torch) -> dict:
         t0 = time.perf_counter()
         groups = Reference().group_commuting(n, x[:rows], z[:rows], c[:rows], mode=args.group_mode)
         dt = time.perf_counter() - t0
+        sx, sz = dev(torch, x[:rows]), dev(torch, z[:rows])
+        o2 = np.zeros(rows, np.uintp)
+        s2 = np.zeros(rows, np.uintp)
+        n2 = ctypes.c_size_t()
+        capi.check(L.wg_group_commuting(torch.cuda.current_device(), 2, rows, sx.data_ptr(), sz.data_ptr(), full,
+                                        o2.ctypes.data_as(psz), s2.ctypes.data_as(psz), ctypes.byref(n2), sh))
+        same = [int(v) for v in s2[: n2.value]] == [len(g[2]) for g in groups] and np.array_equal(
+            x[:rows][o2.astype(np.int64)], np.concatenate([g[0] for g in groups]))
+        out["parity"] = {"terms_checked": rows, "groups_equal": bool(same),
+                         "how": "device group_commuting of the reference's sample against the reference core's "
+                                "groups (sizes, members in order); 262,144 terms: tests/test_gpu_fullsize.py"}
         out["cpu_baseline"] = {"value": rows / dt, "unit": "terms/s", "cores": 1, "kind": "reference",
                                "extrapolated": rows < T, **host_cpu(), "sample": f"reference PauliSum::group_commuting(mode={args.group_mode!r}) on the first "
                                          f"{rows} terms ({len(groups)} groups, {dt:.1f} s); the greedy's cost grows "
@@ -580,24 +652,33 @@ def bench_expectation(args, world, rank, torch) -> dict:
     rl = roofline(prof, {"expect_forward_kernel": G * psi_bytes,
                          "expect_adjoint_kernel": G * psi_bytes + (1 << n) * 16}, peak, kind)
     del res
-    out_cpu = None
+    out_cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # reference expectation_statevector_complex128 (forward only: the
         # reference has no gradient) on the first k terms, scaled to all T
         from oracle import Reference
 
         k = args.cpu_terms
-        hpsi = psi.to(torch.complex128).cpu().numpy()
+        hpsi = psi.to(torch.complex128).cpu().numpy() if not args.c64 else psi.cpu().numpy()
         x, z, c = op[1][:k], op[2][:k], op[3][:k]
         t0 = time.perf_counter()
         Reference().expectation(n, x, z, c, hpsi)
         per_term = (time.perf_counter() - t0) / k
+        from oracle import Oracle
+
+        _, ev, _ = plan.run(psi, terms=True)
+        ev = ev.cpu().numpy()
+        sample = np.random.default_rng(4).choice(len(op[3]), size=16, replace=False)
+        err = float(np.max(np.abs(ev[sample] - Oracle().term_expectations(n, op[1][sample], op[2][sample], hpsi))))
+        parity = {"terms_checked": 16, "max_abs_err": err, "tolerance": 1e-12,
+                  "how": "dE/dc_k = <psi|P_k|psi> of 16 random terms against the FP64 oracle on the same stored "
+                         "amplitudes; 64 terms, H psi and finite differences: tests/test_gpu_fullsize.py"}
         out_cpu = {"value": 1.0 / (per_term * len(op[3])), "unit": "evals/s", "cores": 1, "kind": "reference",
                    "extrapolated": True, **host_cpu(), "sample": f"reference expectation_statevector_complex128 on the first {k} of {len(op[3])} terms "
                              f"({per_term:.3f} s per term), scaled to all terms; forward only (no gradient in "
                              f"the reference)"}
     return {"metric": "E+grad evals/s" if not args.forward_only else "E evals/s", "value": world * 1e3 / t,
-            "unit": "evals/s", "ms_per_step": t, "cpu_baseline": out_cpu,
+            "unit": "evals/s", "ms_per_step": t, "cpu_baseline": out_cpu, "parity": parity,
             "config": {"workload": f"config4: {n} qubits, {len(op[3])} terms, {G} x-groups, "
                                    f"{'c64' if args.c64 else 'c128'} psi, forward{'' if args.forward_only else '+adjoint'}",
                        "byte_model_bytes_per_step": G * psi_bytes + (0 if args.forward_only else 2 * psi_bytes + G * psi_bytes)},
@@ -633,9 +714,57 @@ def bench_batched(args, world, rank, torch) -> dict:
 
     pc_total, _, _, _ = timed_steps(torch, max(1, args.steps // 2), 1, per_call)
     pc = pc_total / max(1, args.steps // 2)
+
+    # the plain per-call drop-in: wg_expectation (the path behind
+    # DevicePauliSum.expectation_statevector) builds its plan on every call and
+    # returns E only -- no gradient, so it does less than a batched evaluation
+    import ctypes as ct
+
+    from wolfgang_b200 import capi
+    from wolfgang_b200.workloads import uneven_pair_operator as _upo
+
+    L = capi.lib()
+    dv = torch.cuda.current_device()
+    dops = []
+    for n, T, seed in pairs:
+        _, x, z, c = _upo(n, T, seed)
+        dops.append((n, T, dev(torch, x), dev(torch, z), dev(torch, c)))
+    val = (ct.c_double * 2)()
+
+    def one_shot():
+        for (n, T, dx, dz, dc), ps in zip(dops, psis):
+            capi.check(L.wg_expectation(dv, n, T, dx.data_ptr(), dz.data_ptr(), dc.data_ptr(), ps.data_ptr(),
+                                        capi.WG_DTYPE_C64 if args.c64 else capi.WG_DTYPE_C128, val, None))
+
+    one_shot()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    one_shot()
+    torch.cuda.synchronize()
+    os_ms = 1e3 * (time.perf_counter() - t0)
     npairs = len(pairs) * world
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # parity: E and dE/dc of the 16 smallest pairs against the FP64 oracle
+        # (all 512 pairs: tests/test_gpu_fullsize.py)
+        from oracle import Oracle
+
+        orc = Oracle()
+        batch.run()
+        torch.cuda.synchronize()
+        small = sorted(range(len(pairs)), key=lambda i: pairs[i][1] << pairs[i][0])[:16]
+        e_err = t_err = 0.0
+        for i in small:
+            n, T, seed = pairs[i]
+            _, x, z, c = uneven_pair_operator(n, T, seed)
+            ps = psis[i].cpu().numpy()
+            E = complex(batch.values[i, 0].item(), batch.values[i, 1].item())
+            e_err = max(e_err, abs(E - orc.expectation(n, x, z, c, ps)) / max(1.0, abs(E)))
+            ev = batch.term_values[i][:T].cpu().numpy()
+            t_err = max(t_err, float(np.max(np.abs(ev - orc.term_expectations(n, x, z, ps)))))
+        parity = {"pairs_checked": 16, "max_rel_err_E": e_err, "max_abs_err_dE_dc": t_err, "tolerance_rel": 1e-10,
+                  "how": f"{'complex64' if args.c64 else 'complex128'} states, FP64 oracle on the same stored "
+                         "amplitudes"}
         # reference expectation (forward only) per term measured at a few qubit
         # counts on this config's own operators; every pair's time estimated
         # as T * 2^n * (time per amplitude at the nearest probed size)
@@ -665,9 +794,307 @@ def bench_batched(args, world, rank, torch) -> dict:
             "config": {"workload": f"config5: {npairs} uneven (H, psi) pairs, n in [8,24], T log-uniform "
                                    f"[100,50000], {'c64' if args.c64 else 'c128'}, forward+gradient, one CUDA graph",
                        "per_call_evals_per_s": len(pairs) / (pc * 1e-3), "per_call_ms": pc,
-                       "batched_over_per_call": pc / t},
+                       "batched_over_per_call": pc / t,
+                       "per_call_path": "one ExpectationPlan.run(terms, H psi) per pair, plans built once",
+                       "one_shot_ms": os_ms, "batched_over_one_shot": os_ms / t,
+                       "one_shot_path": "wg_expectation per pair (DevicePauliSum.expectation_statevector's path: "
+                                        "plan built per call, E only)"},
+            "parity": parity,
             "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+
+
+def bench_products_batch(args, world, rank, torch) -> dict:
+    """Batched uneven products: 256 products A_p * B_p (64 qubits, 16-4,096
+    terms a side) prepared once and replayed from a CUDA graph, against the
+    plain per-call GPU path (one wg_pauli_products per pair)."""
+    import ctypes as ct
+
+    from wolfgang_b200 import capi
+    from wolfgang_b200.products import ProductsBatch
+    from wolfgang_b200.workloads import uneven_product_operands, uneven_product_pairs
+
+    descs = uneven_product_pairs(args.pairs if args.pairs != 512 else 256)
+    if world > 1:
+        descs = shard(descs, rank, world)
+    pairs = [uneven_product_operands(*d) for d in descs]
+    P = sum(len(A[3]) * len(B[3]) for A, B in pairs)
+    dv = torch.cuda.current_device()
+    L = capi.lib()
+    ops = [([dev(torch, v) for v in A[1:]], [dev(torch, v) for v in B[1:]]) for A, B in pairs]
+    w = (pairs[0][0][0] + 63) // 64
+
+    def per_call():
+        for (A, B), (a, b) in zip(pairs, ops):
+            ox, oz, oc, U = ct.c_void_p(), ct.c_void_p(), ct.c_void_p(), ct.c_size_t()
+            capi.check(L.wg_pauli_products(dv, w, a[0].data_ptr(), a[1].data_ptr(), a[2].data_ptr(), len(A[3]),
+                                           b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), len(B[3]),
+                                           capi.WG_PRODUCTS_SIMPLIFY, 1e-12, 0.0, ct.byref(ox), ct.byref(oz),
+                                           ct.byref(oc), ct.byref(U), None))
+            for q in (ox, oz, oc):
+                capi.check(L.wg_free(dv, q, None))
+
+    per_call()  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    per_call()
+    torch.cuda.synchronize()
+    per_call_ms = 1e3 * (time.perf_counter() - t0)
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch = ProductsBatch([((A[0], a[0], a[1], a[2]), (B[0], b[0], b[1], b[2])) for (A, B), (a, b) in zip(pairs, ops)])
+    torch.cuda.synchronize()
+    create_ms = 1e3 * (time.perf_counter() - t0)
+    batch.capture()
+    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, batch.replay)
+    t = max_over_ranks(total, world) / args.steps
+    peak, kind = peaks()
+    rl = roofline(prof, {"pbatch_sums_kernel": 4 * batch.n_products + 24 * batch.n_keys,
+                         "pbatch_write_kernel": batch.n_keys * 12 + batch.n_keys * (16 * w + 16)}, peak, kind)
+    out = {"metric": "batched products terms/s", "value": world * P / (t * 1e-3), "unit": "terms/s",
+           "ms_per_step": t,
+           "config": {"workload": f"{len(pairs) * world} uneven products A_p*B_p, 64 qubits, 16-4096 terms a side, "
+                                  "k-local w in 1..6, matmul+simplify(atol=1e-12), one CUDA graph replay",
+                      "products": P, "keys": batch.n_keys, "per_call_ms": per_call_ms,
+                      "per_call_path": "wg_pauli_products per pair (plan-free drop-in, synchronising)",
+                      "create_ms": create_ms, "batched_over_per_call": per_call_ms / t,
+                      "first_use_over_per_call": per_call_ms / (create_ms + t),
+                      "note": "create sorts every product's key once (the symbolic pass); a replay forms, sums and "
+                              "culls the coefficients"},
+           "roofline": rl, "gpu_launches": launches, "clocks": clocks,
+           "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import Oracle, Reference
+
+        # parity: every pair's result bit for bit against the oracle, on the
+        # smallest pairs and every 16th pair
+        orc = Oracle()
+        got = batch.results()
+        check = sorted(range(len(pairs)), key=lambda i: len(pairs[i][0][3]) * len(pairs[i][1][3]))[:8]
+        check += list(range(0, len(pairs), 16))
+        exact = True
+        for i in sorted(set(check)):
+            A, B = pairs[i]
+            raw = orc.matmul(A[0], A[1:], B[1:], simplify=False)
+            want = orc.simplify(A[0], *raw, 1e-12, 0.0)
+            exact = exact and all(np.ascontiguousarray(g).tobytes() == np.ascontiguousarray(wv).tobytes()
+                                  for g, wv in zip(got[i], want))
+        out["parity"] = {"pairs_checked": len(set(check)), "bit_exact": bool(exact), "max_abs_err": 0.0 if exact else None}
+        ref = Reference()
+        sample = list(range(0, len(pairs), 8))
+        t0 = time.perf_counter()
+        prods = 0
+        for i in sample:
+            A, B = pairs[i]
+            ref.matmul(A[0], A[1:], B[1:], simplify=True, max_intermediate_terms=max(1, len(A[3]) * len(B[3])))
+            prods += len(A[3]) * len(B[3])
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": prods / dt, "unit": "terms/s", "cores": 1, "kind": "reference",
+                               "extrapolated": True, **host_cpu(),
+                               "sample": f"reference PauliSum::matmul(simplify=True) on every 8th pair "
+                                         f"({len(sample)} pairs, {prods} products, {dt:.1f} s)"}
+    batch.close()
+    return out
+
+
+# ---------------------------------------------------------------- per-op comparison with the reference GPU path
+
+# Device-resident operations timed on both sides (this repository: --workload
+# ops; the reference's own CUDA path: --impl reference-gpu), each on seeded
+# inputs both arms regenerate identically:
+#   hh_simplify      config 1: H @ H with simplify (4,096 x 4,096 terms, 20 qubits)
+#   simplify_5e6     simplify of 5,000,000 terms on 20 qubits drawn from 100,000
+#                    distinct keys (98 % duplicates)
+#   commute_4096     config 1: the 4,096 x 4,096 commutation flags (uint8 output)
+#   commute_16384    config 3's first 16,384 terms: the 16,384^2 flags (uint8)
+#   expect_20q       config 1: <psi|H|psi>, 2^20 amplitudes, 4,096 terms
+#   products_config2 config 2: 32,768 x 16,384 products + simplify (5.4e8 products)
+#   expect_26q       config 4: <psi|H|psi>, 2^26 amplitudes, 20,000 terms
+OPS = ("hh_simplify", "simplify_5e6", "commute_4096", "commute_16384", "expect_20q", "products_config2",
+       "expect_26q")
+
+
+def ops_input(W, op):
+    """Seeded inputs of one comparison operation (numpy; both arms)."""
+    if op in ("hh_simplify", "commute_4096", "expect_20q"):
+        (n, x, z, c), psi = W.hamiltonian_20q_and_state()
+        return n, x, z, c, psi
+    if op == "simplify_5e6":
+        rng = np.random.default_rng(W.SEED_BASE + 11)
+        n, px, pz, _ = W.bernoulli_operator(rng, 20, 100_000, 0.25)
+        pick = rng.integers(0, 100_000, size=5_000_000)
+        c = (rng.normal(size=5_000_000) + 1j * rng.normal(size=5_000_000)).astype(np.complex128)
+        return n, px[pick], pz[pick], c, None
+    if op == "commute_16384":
+        n, x, z, c = W.sparse_operator_128q()
+        return n, x[:16384], z[:16384], c[:16384], None
+    if op == "products_config2":
+        return W.klocal_pair_100q()
+    if op == "expect_26q":
+        n, x, z, c = W.xpattern_operator(n=26)
+        return n, x, z, c, W.state_26q()
+    raise ValueError(op)
+
+
+def _host_timed(warmup, reps, call):
+    for _ in range(warmup):
+        call()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        call()
+    return 1e3 * (time.perf_counter() - t0) / max(reps, 1)
+
+
+def bench_ops(args, world, rank, torch) -> dict:
+    """This repository's side of the per-op comparison (device-resident: the
+    operands are on the device before timing; each call synchronises)."""
+    import ctypes as ct
+
+    from wolfgang_b200 import capi
+
+    W = load_workloads()
+    L = capi.lib()
+    dv = torch.cuda.current_device()
+    res = {}
+    for op in [o for o in args.ops.split(",") if o]:
+        reps = 1 if op in ("expect_26q", "products_config2") else args.steps
+        inp = ops_input(W, op)
+        if op in ("hh_simplify", "products_config2"):
+            if op == "hh_simplify":
+                n, x, z, c, _ = inp
+                A = B = (n, x, z, c)
+            else:
+                A, B = inp
+            n, w = A[0], (A[0] + 63) // 64
+            a = [dev(torch, v) for v in A[1:]]
+            b = [dev(torch, v) for v in B[1:]]
+            out = {}
+
+            def call():
+                ox, oz, oc, U = ct.c_void_p(), ct.c_void_p(), ct.c_void_p(), ct.c_size_t()
+                capi.check(L.wg_pauli_products(dv, w, a[0].data_ptr(), a[1].data_ptr(), a[2].data_ptr(), len(A[3]),
+                                               b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), len(B[3]),
+                                               capi.WG_PRODUCTS_SIMPLIFY, 1e-12, 0.0, ct.byref(ox), ct.byref(oz),
+                                               ct.byref(oc), ct.byref(U), None))
+                out["terms"] = U.value
+                for q in (ox, oz, oc):
+                    capi.check(L.wg_free(dv, q, None))
+
+            ms = _host_timed(1, reps, call)
+            res[op] = {"ms": ms, "terms": out["terms"], "products": len(A[3]) * len(B[3])}
+        elif op == "simplify_5e6":
+            n, x, z, c, _ = inp
+            d = [dev(torch, v) for v in (x, z, c)]
+            out = {}
+
+            def call():
+                ox, oz, oc, U = ct.c_void_p(), ct.c_void_p(), ct.c_void_p(), ct.c_size_t()
+                capi.check(L.wg_simplify(dv, 1, len(c), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 1e-12,
+                                         0.0, ct.byref(ox), ct.byref(oz), ct.byref(oc), ct.byref(U), None))
+                out["terms"] = U.value
+                for q in (ox, oz, oc):
+                    capi.check(L.wg_free(dv, q, None))
+
+            res[op] = {"ms": _host_timed(1, reps, call), "terms": out["terms"], "input_terms": len(c)}
+        elif op.startswith("commute"):
+            n, x, z, _, _ = inp
+            T = len(x)
+            w = (n + 63) // 64
+            d = [dev(torch, v) for v in (x, z)]
+            pitch = (T + 31) // 32
+            bits = torch.empty(T * pitch, dtype=torch.int32, device="cuda")
+            flags = torch.empty(T * T, dtype=torch.uint8, device="cuda")
+
+            def bits_call():
+                capi.check(L.wg_commutation_bits(dv, w, d[0].data_ptr(), d[1].data_ptr(), T, d[0].data_ptr(),
+                                                 d[1].data_ptr(), T, bits.data_ptr(), pitch, 0, None))
+                torch.cuda.synchronize()
+
+            def u8_call():
+                capi.check(L.wg_commutation_bits(dv, w, d[0].data_ptr(), d[1].data_ptr(), T, d[0].data_ptr(),
+                                                 d[1].data_ptr(), T, bits.data_ptr(), pitch, 0, None))
+                capi.check(L.wg_bits_to_u8(dv, bits.data_ptr(), T, T, pitch, flags.data_ptr(), None))
+                torch.cuda.synchronize()
+
+            ms_bits = _host_timed(1, reps, bits_call)
+            ms_u8 = _host_timed(1, reps, u8_call)
+            res[op] = {"ms": ms_u8, "ms_bits_only": ms_bits, "commuting": int(flags.sum(dtype=torch.int64).item())}
+        else:  # expectation: the one-shot drop-in (plan built per call) and a reused plan
+            from wolfgang_b200.expectation import ExpectationPlan
+
+            n, x, z, c, psi = inp
+            dx, dz, dc, dpsi = (dev(torch, v) for v in (x, z, c, psi))
+            val = (ct.c_double * 2)()
+
+            def one_shot():
+                capi.check(L.wg_expectation(dv, n, len(c), dx.data_ptr(), dz.data_ptr(), dc.data_ptr(),
+                                            dpsi.data_ptr(), capi.WG_DTYPE_C128, val, None))
+
+            plan = ExpectationPlan((n, x, z, c))
+
+            def reuse():
+                r, _, _ = plan.run(dpsi)
+                torch.cuda.synchronize()
+
+            res[op] = {"ms": _host_timed(1, reps, one_shot), "ms_plan_reused": _host_timed(1, reps, reuse),
+                       "value": [val[0], val[1]]}
+            plan.close()
+        torch.cuda.empty_cache()
+    return {"metric": "device-resident ms per call (sum over ops)", "value": sum(v["ms"] for v in res.values()),
+            "unit": "ms", "higher_is_better": False, "ms_per_step": sum(v["ms"] for v in res.values()),
+            "config": {"workload": "per-op comparison set (bench.OPS): " + args.ops,
+                       "timing": "host clock around each synchronising call, operands resident on the device",
+                       "ops": res},
+            "gpu_launches": None}
+
+
+def reference_gpu_arm(args) -> dict:
+    """The reference's own CUDA path (its DevicePauliSum, src/cuda/*.cu built
+    for sm_100a, oracle/_ref/libwgref_cuda.so) on the same operations and
+    GPU, device-resident, timed by the host clock around each of its
+    synchronising calls.  Loads no library of this repository."""
+    from oracle import ReferenceGPU
+
+    if not ReferenceGPU.available():
+        return {"impl": "reference-gpu", "unavailable": "oracle/_ref/libwgref_cuda.so was not built"}
+    ref = ReferenceGPU()
+    W = load_workloads()
+    res = {}
+    for op in [o for o in args.ops.split(",") if o]:
+        reps = 1 if op in ("expect_26q", "products_config2") else args.steps
+        inp = ops_input(W, op)
+        try:
+            if op in ("hh_simplify", "products_config2"):
+                if op == "hh_simplify":
+                    n, x, z, c, _ = inp
+                    A = B = (n, x, z, c)
+                else:
+                    A, B = inp
+                P = len(A[3]) * len(B[3])
+                ms, terms = ref.matmul(A[0], A[1:], B[1:], True, max(P, 50_000_000), 1, reps)
+                res[op] = {"ms": ms, "terms": terms, "products": P}
+            elif op == "simplify_5e6":
+                n, x, z, c, _ = inp
+                ms, terms = ref.simplify(n, x, z, c, 1e-12, 0.0, 1, reps)
+                res[op] = {"ms": ms, "terms": terms, "input_terms": len(c)}
+            elif op.startswith("commute"):
+                n, x, z, _, _ = inp
+                ms, count = ref.commutes_device(n, (x, z), (x, z), 1, reps)
+                res[op] = {"ms": ms, "commuting": count}
+            else:
+                n, x, z, c, psi = inp
+                ms, v = ref.expectation(n, x, z, c, psi, 1 if reps > 1 else 0, reps)
+                res[op] = {"ms": ms, "value": [v.real, v.imag]}
+        except Exception as exc:  # the reference's own refusal (e.g. out of memory) is reported, not hidden
+            res[op] = {"error": str(exc)}
+    return {"impl": "reference-gpu", "metric": "device-resident ms per call (sum over ops)",
+            "value": sum(v.get("ms", 0.0) for v in res.values()), "unit": "ms", "higher_is_better": False,
+            "config": {"workload": "per-op comparison set (bench.OPS): " + args.ops,
+                       "timing": "host clock around each synchronising call of the reference's DevicePauliSum, "
+                                 "operands uploaded once beforehand",
+                       "build": "reference src/cuda/*.cu, nvcc 12.9 -O2 -gencode arch=compute_100a,code=sm_100a",
+                       "ops": res}}
 
 
 def reference_arm(args, world, rank) -> dict:
@@ -706,9 +1133,10 @@ def build_parser() -> argparse.ArgumentParser:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["products", "commutation", "grouping", "expectation", "batched"],
-                    default="products")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
+    ap.add_argument("--workload", choices=["products", "commutation", "grouping", "expectation", "batched",
+                                           "products_batch", "ops"], default="products")
+    ap.add_argument("--ops", default=",".join(OPS), help="operations of --workload ops / --impl reference-gpu")
     ap.add_argument("--group-mode", choices=["qwc", "full"], default="qwc", help="grouping mode (config 3)")
     ap.add_argument("--cpu-group-terms", type=int, default=16384, help="reference terms timed for grouping")
     ap.add_argument("--terms", type=int, default=262144, help="commutation terms (config 3)")
@@ -732,6 +1160,14 @@ def main() -> None:
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
 
+    if args.impl == "reference-gpu":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        out = reference_gpu_arm(args)
+        out.update(n_gpus=1, steps=args.steps, warmup=args.warmup, data="synthetic (seeded generators)")
+        print(json.dumps(out), flush=True)
+        return
+
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
@@ -747,9 +1183,11 @@ def main() -> None:
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     fn = {"products": bench_products, "commutation": bench_commutation, "grouping": bench_grouping,
-          "expectation": bench_expectation, "batched": bench_batched}[args.workload]
+          "expectation": bench_expectation, "batched": bench_batched, "products_batch": bench_products_batch,
+          "ops": bench_ops}[args.workload]
     out = fn(args, world, rank, torch)
-    out.update(n_gpus=world, steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling="weak",
+    out.setdefault("higher_is_better", True)
+    out.update(n_gpus=world, steps=args.steps, warmup=args.warmup, scaling="weak",
                vs_baseline=None, dtype="u64" if args.workload in ("commutation", "grouping") else "f64",
                data=f"synthetic (seeded generator, workload {args.workload})")
     if rank == 0:

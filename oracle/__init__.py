@@ -5,6 +5,10 @@
 * ``Reference`` wraps ``_ref/libwgref.so``, the reference's own CPU core compiled
   from its sources by ``Makefile`` (when the reference checkout was available
   at build time; the prebuilt library travels with the repository snapshot).
+* ``ReferenceGPU`` wraps ``_ref/libwgref_cuda.so``, the reference's own CUDA
+  path (src/cuda/*.cu built for sm_100a) with its CPU core, for timing it on
+  the same GPU; it defines the reference's DevicePauliSum, so it is never
+  loaded into a process that loads this repository's C++ layer.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline /
 reference arm may import this package.  The product (``wolfgang_b200``) never
@@ -26,6 +30,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libwgref.so"
+REF_GPU_SO = HERE / "_ref" / "libwgref_cuda.so"
 
 _sz = ctypes.c_size_t
 _p = ctypes.c_void_p
@@ -338,3 +343,75 @@ class Reference:
         buf = ctypes.create_string_buffer(512)
         self._check(self.lib.wgref_cpu_backend(buf, _sz(512)))
         return buf.value.decode()
+
+
+class ReferenceGPU:
+    """The reference's DevicePauliSum path on the GPU (ref_gpu_shim.cpp).
+
+    Every method uploads the operands once, makes `warmup` untimed and `reps`
+    timed calls of the reference's stock device-resident operation (each call
+    synchronises before it returns) and returns (mean ms per call, result)."""
+
+    def __init__(self, path: Path = REF_GPU_SO) -> None:
+        if not path.exists():
+            raise FileNotFoundError(f"{path} was not built (reference sources unavailable)")
+        self.lib = ctypes.CDLL(str(path), mode=os.RTLD_LOCAL)
+        self.lib.wgrefgpu_last_error.restype = ctypes.c_char_p
+
+    @staticmethod
+    def available() -> bool:
+        return REF_GPU_SO.exists()
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise OracleError(self.lib.wgrefgpu_last_error().decode())
+
+    def matmul(self, n, lhs, rhs, simplify=True, max_intermediate_terms=50_000_000, warmup=1, reps=3):
+        lx, lz, lc = lhs
+        rx, rz, rc = rhs
+        w = words_for(n)
+        nl, nr = len(lc), len(rc)
+        lx, lz, lc = _u64(lx, nl, w), _u64(lz, nl, w), _c128(lc, nl)
+        rx, rz, rc = _u64(rx, nr, w), _u64(rz, nr, w), _c128(rc, nr)
+        ms, terms = ctypes.c_double(), _sz()
+        self._check(self.lib.wgrefgpu_matmul(_sz(n), _sz(nl), _sz(nr), _sz(w), _p(_ptr(lx)), _p(_ptr(lz)),
+                                             _p(_ptr(lc)), _p(_ptr(rx)), _p(_ptr(rz)), _p(_ptr(rc)),
+                                             ctypes.c_int(int(simplify)), _sz(max_intermediate_terms),
+                                             ctypes.c_int(warmup), ctypes.c_int(reps), ctypes.byref(ms),
+                                             ctypes.byref(terms)))
+        return ms.value, terms.value
+
+    def simplify(self, n, x, z, c, atol=1e-12, rtol=0.0, warmup=1, reps=3):
+        T = len(c)
+        w = words_for(n)
+        x, z, c = _u64(x, T, w), _u64(z, T, w), _c128(c, T)
+        ms, terms = ctypes.c_double(), _sz()
+        self._check(self.lib.wgrefgpu_simplify(_sz(n), _sz(T), _sz(w), _p(_ptr(x)), _p(_ptr(z)), _p(_ptr(c)),
+                                               ctypes.c_double(atol), ctypes.c_double(rtol), ctypes.c_int(warmup),
+                                               ctypes.c_int(reps), ctypes.byref(ms), ctypes.byref(terms)))
+        return ms.value, terms.value
+
+    def commutes_device(self, n, lhs, rhs, warmup=1, reps=3):
+        w = words_for(n)
+        lx, lz = lhs[0], lhs[1]
+        rx, rz = rhs[0], rhs[1]
+        nl, nr = len(lx), len(rx)
+        lx, lz = _u64(lx, nl, w), _u64(lz, nl, w)
+        rx, rz = _u64(rx, nr, w), _u64(rz, nr, w)
+        ms, count = ctypes.c_double(), ctypes.c_uint64()
+        self._check(self.lib.wgrefgpu_commutes_device(_sz(n), _sz(nl), _sz(nr), _sz(w), _p(_ptr(lx)), _p(_ptr(lz)),
+                                                      _p(_ptr(rx)), _p(_ptr(rz)), _sz(nl * nr), ctypes.c_int(warmup),
+                                                      ctypes.c_int(reps), ctypes.byref(ms), ctypes.byref(count)))
+        return ms.value, count.value
+
+    def expectation(self, n, x, z, c, psi, warmup=1, reps=3):
+        T = len(c)
+        w = words_for(n)
+        x, z, c = _u64(x, T, w), _u64(z, T, w), _c128(c, T)
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        ms = ctypes.c_double()
+        out = np.zeros(2, np.float64)
+        self._check(self.lib.wgrefgpu_expectation(_sz(n), _sz(T), _sz(w), _p(_ptr(x)), _p(_ptr(z)), _p(_ptr(c)),
+                                                  _p(_ptr(psi)), ctypes.c_int(warmup), ctypes.c_int(reps),
+                                                  ctypes.byref(ms), _p(_ptr(out))))
+        return ms.value, complex(out[0], out[1])

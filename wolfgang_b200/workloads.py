@@ -15,6 +15,9 @@ machine regenerates the same inputs; no dataset is read.
      patterns (weight a in 0..4), term weight U{1..8}.
   5  batched: 512 (H, psi) pairs, n in U{8..24}, T log-uniform in
      [100, 50,000], weight U{1..6}, real N(0,1) coefficients.
+  6  batched products: 256 products A_p * B_p on 64 qubits, term counts
+     log-uniform in [16, 4,096] on each side, weight U{1..6}, complex N(0,1)
+     coefficients (the product counterpart of 5).
 """
 
 from __future__ import annotations
@@ -151,3 +154,16 @@ def uneven_pair_operator(n: int, T: int, seed: int):
 
 def uneven_pair_state(n: int, seed: int, dtype=np.complex128) -> np.ndarray:
     return random_state(np.random.default_rng(seed + 1_000_000), n, dtype)
+
+
+def uneven_product_pairs(count: int = 256, n: int = 64, t_min: int = 16, t_max: int = 4096):
+    """List of (n, T_lhs, T_rhs, seed) descriptors of uneven products."""
+    rng = rng_for(6)
+    Ts = np.round(np.exp(rng.uniform(np.log(t_min), np.log(t_max), size=(count, 2)))).astype(np.int64)
+    return [(n, int(a), int(b), SEED_BASE + 6000 + i) for i, (a, b) in enumerate(Ts)]
+
+
+def uneven_product_operands(n: int, t_lhs: int, t_rhs: int, seed: int):
+    rng = np.random.default_rng(seed)
+    weights = np.arange(1, min(6, n) + 1)
+    return klocal_operator(rng, n, t_lhs, weights), klocal_operator(rng, n, t_rhs, weights)
