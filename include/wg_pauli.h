@@ -131,9 +131,12 @@ int wg_profile_report(char* buf, size_t cap);
  * (include/wolfgang/pauli_sum.hpp:77-79).
  * bits[row*pitch_words + c/32] bit (c%32) = 1 iff lhs term `row` commutes with
  * rhs term c; pitch_words >= ceil(n_rhs/32); padding bits are written 0.
- * algo: 0 = autotuned choice, 1 = popcount/LOP3 with warp-ballot packing,
- * 2 = bit-plane XOR over the lhs support (up to 256 qubits; above that the
- * call uses 1).  All algos give identical bits. */
+ * algo: 0 = the autotuner's choice for the shape class (kernel, tile, rows
+ * per CTA; see wg_autotune_set_mode), else a rule on the sizes and the word
+ * count -- no term data is read, so the choice costs no synchronisation;
+ * 1 = popcount/LOP3 with warp-ballot packing; 2 = bit-plane XOR over the lhs
+ * support (up to 256 qubits; above that the call uses 1).  All algos give
+ * identical bits. */
 int wg_commutation_bits(int device, size_t words, const uint64_t* lhs_x,
                         const uint64_t* lhs_z, size_t n_lhs, const uint64_t* rhs_x,
                         const uint64_t* rhs_z, size_t n_rhs, uint32_t* bits,
