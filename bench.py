@@ -691,7 +691,7 @@ def bench_batched(args, world, rank, torch) -> dict:
     from wolfgang_b200.expectation import ExpectationBatch, ExpectationPlan
     from wolfgang_b200.workloads import uneven_pair_operator, uneven_pairs
 
-    pairs = uneven_pairs(args.pairs)
+    pairs = uneven_pairs(args.pairs, n_min=args.min_qubits, n_max=args.max_qubits)
     if world > 1:
         pairs = shard(pairs, rank, world)
     plans, psis = [], []
@@ -702,11 +702,29 @@ def bench_batched(args, world, rank, torch) -> dict:
         gen.manual_seed(seed)
         p = torch.randn(1 << n, dtype=torch.complex128, device="cuda", generator=gen)
         psis.append((p / torch.linalg.vector_norm(p)).to(dtype))
-    batch = ExpectationBatch(plans, psis, gradients=True)
-    batch.capture()
+    from wolfgang_b200 import capi
 
-    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, batch.replay)
+    amp = 8 if args.c64 else 16
+    fwd_bytes = sum(pl.n_groups * (1 << pl.n) * amp for pl in plans)  # G_x |psi| per pair
+    adj_bytes = fwd_bytes + sum((1 << pl.n) * 16 for pl in plans)      # + H psi written
+    batch = ExpectationBatch(plans, psis, gradients=True)
+    l0 = capi.kernel_launches()
+    batch.capture()  # one direct run, then the captured one
+    per_run = (capi.kernel_launches() - l0) // 2
+
+    total, _, _, clocks = timed_steps(torch, args.steps, args.warmup, batch.replay)
     t = max_over_ranks(total, world) / args.steps
+    launches = per_run * args.steps  # kernels each replay launches, times the timed replays
+    # per-kernel times: a replay records no library events, so one run is
+    # launched directly with the profiler on (outside the timed region)
+    _, prof, _, _ = timed_steps(torch, 1, 0, batch.run)
+    # the same batch without gradients (E and dE/dc only), for the E-only
+    # per-call comparison below
+    fwd = ExpectationBatch(plans, psis, gradients=False)
+    fwd.capture()
+    fwd_total, _, _, _ = timed_steps(torch, max(1, args.steps // 2), 1, fwd.replay)
+    fwd_ms = fwd_total / max(1, args.steps // 2)
+    fwd.close()
 
     def per_call():
         for pl, ps in zip(plans, psis):
@@ -720,7 +738,6 @@ def bench_batched(args, world, rank, torch) -> dict:
     # returns E only -- no gradient, so it does less than a batched evaluation
     import ctypes as ct
 
-    from wolfgang_b200 import capi
     from wolfgang_b200.workloads import uneven_pair_operator as _upo
 
     L = capi.lib()
@@ -791,14 +808,18 @@ def bench_batched(args, world, rank, torch) -> dict:
                          "estimated as T * 2^n * (ns per amplitude at the nearest probed size); forward only (no gradient in the "
                          f"reference); {est:.0f} s estimated for the batch"}
     return {"metric": "batched E+grad evals/s", "value": npairs / (t * 1e-3), "unit": "evals/s", "ms_per_step": t,
-            "config": {"workload": f"config5: {npairs} uneven (H, psi) pairs, n in [8,24], T log-uniform "
+            "config": {"workload": f"config5: {npairs} uneven (H, psi) pairs, n in [{args.min_qubits},{args.max_qubits}], T log-uniform "
                                    f"[100,50000], {'c64' if args.c64 else 'c128'}, forward+gradient, one CUDA graph",
                        "per_call_evals_per_s": len(pairs) / (pc * 1e-3), "per_call_ms": pc,
                        "batched_over_per_call": pc / t,
                        "per_call_path": "one ExpectationPlan.run(terms, H psi) per pair, plans built once",
-                       "one_shot_ms": os_ms, "batched_over_one_shot": os_ms / t,
+                       "one_shot_ms": os_ms, "batched_forward_ms": fwd_ms,
+                       "batched_forward_over_one_shot": os_ms / fwd_ms,
                        "one_shot_path": "wg_expectation per pair (DevicePauliSum.expectation_statevector's path: "
-                                        "plan built per call, E only)"},
+                                        "plan built per call, E only), against the batch without gradients",
+                       "qubits": f"{args.min_qubits}..{args.max_qubits}"},
+            "roofline": roofline(prof, {"expect_forward_kernel": fwd_bytes, "expect_adjoint_kernel": adj_bytes},
+                                 *peaks()),
             "parity": parity,
             "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
@@ -846,9 +867,15 @@ def bench_products_batch(args, world, rank, torch) -> dict:
     batch = ProductsBatch([((A[0], a[0], a[1], a[2]), (B[0], b[0], b[1], b[2])) for (A, B), (a, b) in zip(pairs, ops)])
     torch.cuda.synchronize()
     create_ms = 1e3 * (time.perf_counter() - t0)
-    batch.capture()
-    total, prof, launches, clocks = timed_steps(torch, args.steps, args.warmup, batch.replay)
+    l0 = capi.kernel_launches()
+    batch.capture()  # one direct run, then the captured one
+    per_run = (capi.kernel_launches() - l0) // 2
+    total, _, _, clocks = timed_steps(torch, args.steps, args.warmup, batch.replay)
     t = max_over_ranks(total, world) / args.steps
+    launches = per_run * args.steps  # kernels each replay launches, times the timed replays
+    # per-kernel times: a replay records no library events, so the same run is
+    # launched directly with the profiler on (outside the timed region)
+    _, prof, _, _ = timed_steps(torch, max(1, args.steps // 2), 1, batch.run)
     peak, kind = peaks()
     rl = roofline(prof, {"pbatch_sums_kernel": 4 * batch.n_products + 24 * batch.n_keys,
                          "pbatch_write_kernel": batch.n_keys * 12 + batch.n_keys * (16 * w + 16)}, peak, kind)
@@ -1045,7 +1072,7 @@ def bench_ops(args, world, rank, torch) -> dict:
             "unit": "ms", "higher_is_better": False, "ms_per_step": sum(v["ms"] for v in res.values()),
             "config": {"workload": "per-op comparison set (bench.OPS): " + args.ops,
                        "timing": "host clock around each synchronising call, operands resident on the device",
-                       "ops": res},
+                       "sort": args.sort, "ops": res},
             "gpu_launches": None}
 
 
@@ -1145,11 +1172,15 @@ def build_parser() -> argparse.ArgumentParser:
     ap.add_argument("--c64", action="store_true", help="complex64 statevector storage")
     ap.add_argument("--forward-only", action="store_true")
     ap.add_argument("--pairs", type=int, default=512, help="batched pairs (config 5)")
+    ap.add_argument("--min-qubits", type=int, default=8, help="batched pairs: smallest qubit count")
+    ap.add_argument("--max-qubits", type=int, default=24, help="batched pairs: largest qubit count")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--cpu-terms", type=int, default=8, help="reference terms timed for the expectation baseline")
     ap.add_argument("--ref-rows", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sort", choices=["auto", "lsd", "bucket"], default="auto",
+                    help="sort-reduce algorithm of products and simplify (results identical)")
     ap.add_argument("--lhs-terms", type=int, default=32768, help="A terms (smaller values: profiling cases)")
     ap.add_argument("--rhs-terms", type=int, default=16384, help="B terms")
     return ap
@@ -1182,6 +1213,10 @@ def main() -> None:
 
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
+    if args.sort != "auto":
+        from wolfgang_b200 import capi
+
+        capi.set_sort_algorithm({"lsd": capi.WG_SORT_LSD, "bucket": capi.WG_SORT_BUCKET}[args.sort])
     fn = {"products": bench_products, "commutation": bench_commutation, "grouping": bench_grouping,
           "expectation": bench_expectation, "batched": bench_batched, "products_batch": bench_products_batch,
           "ops": bench_ops}[args.workload]

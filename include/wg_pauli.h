@@ -243,7 +243,9 @@ int wg_products_batch_destroy(wg_products_batch_t batch);
 /* Sort-reduce algorithm behind wg_simplify and the simplifying modes of
  * wg_pauli_products.  No reference counterpart (the reference has one sort);
  * both algorithms give identical results, bit for bit.
- *   WG_SORT_AUTO    (default) bucketed for 1-2 mask words and >= 2^20 items;
+ *   WG_SORT_AUTO    (default) bucketed for 1-2 mask words, >= 2^20 items and
+ *                   keys that vary in more than 8 (one word) or 5 (two words)
+ *                   of their 8-bit digits; LSD otherwise;
  *   WG_SORT_LSD     multi-word LSD radix sort of full keys;
  *   WG_SORT_BUCKET  bucketed sort on 64-bit key codes (1-2 mask words, at most
  *                   255 significant key bits); falls back to WG_SORT_LSD when a

@@ -123,15 +123,29 @@ def test_bucket_klocal_products_match_lsd(cuda, oracle, algo):
     assert same(got, oracle.simplify(100, *raw, 1e-12, 0.0))
 
 
-def test_bucket_hh_20q_operator_auto(cuda, oracle, algo):
-    """H@H of the 4,096-term 20-qubit operator (2^24 products) takes the bucketed path by default."""
+def test_auto_sort_choice_by_key_width(cuda, oracle, algo):
+    """WG_SORT_AUTO: H@H of the 4,096-term 20-qubit operator (2^24 products;
+    keys vary in 6 of their 8-bit digits) takes the LSD pipeline, a 100-qubit
+    k-local product of 2^21 items (keys vary in most digits) the bucketed
+    path; both are bit-exact, and the other algorithm gives the same bits."""
     from wolfgang_b200.workloads import hamiltonian_20q_and_state
 
     (n, x, z, c), _ = hamiltonian_20q_and_state()
     algo(capi.WG_SORT_AUTO)
     got = G.products(n, (x, z, c), (x, z, c), capi.WG_PRODUCTS_SIMPLIFY)
-    assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    assert capi.last_sort_algorithm() == capi.WG_SORT_LSD
     assert same(got, oracle.matmul(n, (x, z, c), (x, z, c), simplify=True))
+    algo(capi.WG_SORT_BUCKET)
+    assert same(got, G.products(n, (x, z, c), (x, z, c), capi.WG_PRODUCTS_SIMPLIFY))
+    assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    rng = seeded("auto-wide")
+    A = klocal(rng, 100, 2048)
+    B = klocal(rng, 100, 1024)
+    algo(capi.WG_SORT_AUTO)
+    got = G.products(100, A[1:], B[1:])
+    assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    raw = oracle.matmul(100, A[1:], B[1:], simplify=False)
+    assert same(got, oracle.simplify(100, *raw, 1e-12, 0.0))
 
 
 def test_bucket_tie_heavy_position_codes(cuda, oracle, algo):
