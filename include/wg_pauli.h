@@ -219,8 +219,9 @@ int wg_pauli_products(int device, size_t words, const uint64_t* lhs_x,
  * between runs; the masks must not) and writes pair p's simplified product,
  * in canonical order, to the batch's output slots (wg_products_batch_result)
  * and its term count to the device array of wg_products_batch_counts.  At
- * most 2^30 products per pair and fewer than 2^32 in all; runs of one batch
- * must not overlap. */
+ * most 2^30 products per pair and fewer than 2^32 in all; coefficient buffers
+ * 16-byte aligned (as every complex128 array is); runs of one batch must not
+ * overlap. */
 typedef struct wg_products_batch_s* wg_products_batch_t;
 int wg_products_batch_create(int device, size_t words, size_t n_pairs, const uint64_t* const* lhs_x,
                              const uint64_t* const* lhs_z, const double* const* lhs_c, const size_t* n_lhs,

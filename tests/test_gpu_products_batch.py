@@ -130,3 +130,44 @@ def test_products_batch_rejects_bad_arguments(cuda):
         ProductsBatch([(A, A)], mode="raw")
     with pytest.raises(ValueError, match="tolerances"):
         ProductsBatch([(A, A)], atol=-1.0)
+
+
+def test_products_batch_rejects_misaligned_coefficients(cuda):
+    import ctypes
+
+    torch = cuda
+    rng = seeded("pbatch-align")
+    A = random_operator(rng, 10, 4, 0.3)
+    x, z = (torch.from_numpy(A[k].view(np.int64)).cuda() for k in (1, 2))
+    c = torch.zeros(2 * len(A[3]) + 1, dtype=torch.float64, device="cuda")  # doubles from an 8-byte offset
+    P = ctypes.c_void_p * 1
+    S = ctypes.c_size_t * 1
+    h = ctypes.c_void_p()
+    with pytest.raises(ValueError, match="16-byte aligned"):
+        capi.call("wg_products_batch_create", 0, 1, 1, P(x.data_ptr()), P(z.data_ptr()), P(c.data_ptr() + 8), S(4),
+                  P(x.data_ptr()), P(z.data_ptr()), P(c.data_ptr() + 8), S(4), capi.WG_PRODUCTS_SIMPLIFY, 1e-12, 0.0,
+                  ctypes.byref(h), None)
+
+
+@pytest.mark.parametrize("rtol", [0.0, 0.2])
+def test_products_batch_nonfinite_and_huge_coefficients(cuda, oracle, rtol):
+    """An infinite |product| makes atol + rtol * max NaN (nothing of that pair
+    survives); NaN products never raise the maximum; huge finite products
+    overflow only where the reference's would."""
+    from wolfgang_b200.products import ProductsBatch
+
+    rng = seeded("pbatch-nonfinite", rtol)
+    n = 16
+    pairs = uneven_pairs(rng, n, 6, pool=40)
+    special = [complex(np.inf, 0.5), complex(np.nan, 1.0), complex(1e200, -1e200), complex(1e300, 0.0)]
+    for k, v in enumerate(special):
+        A, B = pairs[k]
+        c = A[3].copy()
+        c[len(c) // 2] = v
+        pairs[k] = ((A[0], A[1], A[2], c), B)
+    batch = ProductsBatch(pairs, atol=1e-12, rtol=rtol)
+    batch.run()
+    for (A, B), g in zip(pairs, batch.results()):
+        for a, b in zip(g, oracle_pair(oracle, n, A, B, "simplify", 1e-12, rtol)):
+            assert same_bits(a, b)
+    batch.close()

@@ -53,13 +53,23 @@ struct PairMasks {
   uint64_t item_base;  // first product of the pair in the batch
 };
 
-// What a run needs of one pair.
+// What a run needs of one pair.  q / n_r is computed as the high word of
+// q * div_m (div_m = floor((2^64 - 1) / n_r) + 1, exact for q, n_r < 2^32;
+// n_r = 1 divides trivially).
 struct PairNum {
   const double* lc;
   const double* rc;
   uint64_t n_r;
+  uint64_t div_m;
   uint64_t seg_base;  // first segment of the pair = first output slot
   uint64_t n_seg;
+};
+
+// How a run forms each pair's largest |product| (the rtol threshold):
+enum MaxMode : int {
+  kMaxNone = 0,  // fused mode: fixed threshold
+  kMaxInf = 1,   // rtol == 0: atol + 0 * max is atol unless some |product| is infinite
+  kMaxFull = 2,  // rtol > 0: the maximum itself
 };
 
 // ------------------------------------------------------------- symbolic pass
@@ -150,7 +160,9 @@ __global__ void pbatch_count_kernel(const uint32_t* __restrict__ seg_pair, size_
 // right (FP64, no FMA: the reference's rounding); in SIMPLIFY mode the
 // largest |product| of each pair, for the rtol threshold (non-negative
 // doubles order like their bits; a NaN never replaces the running maximum,
-// std::max's rule).
+// std::max's rule) -- with rtol = 0 only the magnitudes that may be infinite
+// (a part beyond 2^1022 or not finite) are formed, since a finite maximum
+// leaves the threshold at atol.
 __global__ void __launch_bounds__(kThreads) pbatch_sums_kernel(
     const PairNum* __restrict__ pairs, const uint32_t* __restrict__ seg_start, const uint32_t* __restrict__ seg_pair,
     const uint32_t* __restrict__ code, size_t S, int want_max, double* __restrict__ segsum,
@@ -166,16 +178,19 @@ __global__ void __launch_bounds__(kThreads) pbatch_sums_kernel(
     if (valid) {
       const PairNum P = pairs[p];
       const uint32_t b = seg_start[s], e = seg_start[s + 1];
+      const uint32_t nr = static_cast<uint32_t>(P.n_r);  // below 2^30
       c128 acc{0.0, 0.0};
       for (uint32_t j = b; j < e; ++j) {
         const uint32_t cj = __ldg(code + j);
-        const uint32_t q = cj >> 2, nr = static_cast<uint32_t>(P.n_r);  // both below 2^30
-        const uint32_t l = q / nr, r = q - l * nr;
-        const c128 a{__ldg(P.lc + 2 * l), __ldg(P.lc + 2 * l + 1)};
-        const c128 bb{__ldg(P.rc + 2 * r), __ldg(P.rc + 2 * r + 1)};
-        const c128 prod = wgd::rotate(wgd::cmul(a, bb), cj & 3u);
+        const uint32_t q = cj >> 2;
+        const uint32_t l = nr == 1 ? q : static_cast<uint32_t>(__umul64hi(static_cast<uint64_t>(q), P.div_m));
+        const uint32_t r = q - l * nr;
+        const double2 av = __ldg(reinterpret_cast<const double2*>(P.lc) + l);
+        const double2 bv = __ldg(reinterpret_cast<const double2*>(P.rc) + r);
+        const c128 prod = wgd::rotate(wgd::cmul(c128{av.x, av.y}, c128{bv.x, bv.y}), cj & 3u);
         acc = wgd::cadd(acc, prod);
-        if (want_max) {
+        if (want_max == kMaxFull ||
+            (want_max == kMaxInf && !(fabs(prod.re) <= 0x1p1022 && fabs(prod.im) <= 0x1p1022))) {
           const double m = wgd::hypot_ref(prod.re, prod.im);
           if (mx < m) mx = m;
         }
@@ -211,7 +226,11 @@ __global__ void pbatch_keep_kernel(const uint32_t* __restrict__ seg_pair, const 
       const double mx = __longlong_as_double(static_cast<long long>(pair_max[seg_pair[s]]));
       thr = __dadd_rn(atol, __dmul_rn(rtol, mx));
     }
-    keep[s] = wgd::hypot_ref(segsum[2 * s], segsum[2 * s + 1]) > thr;
+    // without NaNs the rounded |s| is never below max(|re|, |im|): most sums are
+    // decided without the full hypot
+    const double re = segsum[2 * s], im = segsum[2 * s + 1];
+    const bool plain = !isnan(re) && !isnan(im);
+    keep[s] = (plain && (fabs(re) > thr || fabs(im) > thr)) || wgd::hypot_ref(re, im) > thr;
   }
 }
 
@@ -285,11 +304,15 @@ void build_batch(wg_products_batch_s& b, const uint64_t* const* lhs_x, const uin
                         " has " + std::to_string(P) + "); use wg_pauli_products for it");
     if (P > 0) {
       if (!lhs_c[p] || !rhs_c[p]) wg::throw_invalid("product batch pair has a null coefficient buffer");
+      // runs read a coefficient (re, im) as one 16-byte load
+      if ((reinterpret_cast<uintptr_t>(lhs_c[p]) | reinterpret_cast<uintptr_t>(rhs_c[p])) & 15u)
+        wg::throw_invalid("product batch coefficient buffers must be 16-byte aligned (complex128 arrays)");
       if (W > 0 && (!lhs_x[p] || !lhs_z[p] || !rhs_x[p] || !rhs_z[p]))
         wg::throw_invalid("product batch pair has a null mask buffer");
     }
     masks[p] = PairMasks{lhs_x[p], lhs_z[p], rhs_x[p], rhs_z[p], n_rhs[p], item_base[p]};
-    nums[p] = PairNum{lhs_c[p], rhs_c[p], n_rhs[p], 0, 0};
+    const uint64_t div_m = n_rhs[p] > 1 ? ~0ull / n_rhs[p] + 1 : 0ull;
+    nums[p] = PairNum{lhs_c[p], rhs_c[p], n_rhs[p], div_m, 0, 0};
     item_base[p + 1] = item_base[p] + P;
     if (item_base[p + 1] > 0xffffffffull) wg::throw_invalid("a product batch takes fewer than 2^32 products in all");
   }
@@ -383,12 +406,13 @@ void run_batch(wg_products_batch_s& b, cudaStream_t s) {
     return;
   }
   const bool fused = b.mode == WG_PRODUCTS_FUSED;
+  const int max_mode = fused ? kMaxNone : b.rtol > 0.0 ? kMaxFull : kMaxInf;
   if (!fused)
     wg::check_cuda(cudaMemsetAsync(b.pair_max.get(), 0, sizeof(unsigned long long) * b.n_pairs, s), "clear maxima");
   WG_TIMED("pbatch_sums_kernel", s,
     pbatch_sums_kernel<<<b.sum_blocks, kThreads, 0, s>>>(b.pairs.as<PairNum>(), b.seg_start.as<uint32_t>(),
                                                          b.seg_pair.as<uint32_t>(), b.code.as<uint32_t>(), S,
-                                                         fused ? 0 : 1, b.segsum.as<double>(),
+                                                         max_mode, b.segsum.as<double>(),
                                                          b.pair_max.as<unsigned long long>()));
   wg::check_launch("launch batch sums");
   const unsigned g = wg::grid_for(S, kThreads, device, 8);

@@ -93,7 +93,6 @@ constexpr unsigned kFlagCoarseFull = 8u;        // fallbacks: a coarse region ov
 constexpr unsigned kFlagFineFull = 16u;         //   a fine bucket over kCap items (not of one key),
 constexpr unsigned kFlagDistinct = 32u;         //   a tie of more than kDistinct keys
 constexpr unsigned kFallbackMask = kFlagCoarseFull | kFlagFineFull | kFlagDistinct;
-constexpr unsigned kFlagTimeout = 64u;          // a bulk copy's mbarrier wait ran out (bounded; see output)
 
 struct Control {
   unsigned k2_ticket;
@@ -109,6 +108,7 @@ struct Control {
   unsigned refined;              // fine buckets split again after counting
   unsigned long long phase[4];   // final-kernel cycles per phase (traced runs)
   unsigned long long fphase[5];  // fine-kernel cycles per phase (traced runs)
+  unsigned long long digits[9];  // traced runs: fine buckets by the number of 8-bit code digits that vary
 };
 
 // ------------------------------------------------------------------ keys and codes
@@ -1414,7 +1414,26 @@ __global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src 
       }
       if (tid == 0) S.n_runs = 0;
       __syncthreads();
-      if (P.trace && tid == 0) S.tp[1] = clock64();
+      if (P.trace) {
+        // how many 8-bit digits of the bucket's codes vary (an LSD pass would sort one each)
+        const uint64_t c0 = S.code[pidx(0)];
+        uint64_t v = 0;
+        for (int i = tid; i < n; i += kK3Threads) v |= S.code[pidx(i)] ^ c0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+        uint64_t* red = reinterpret_cast<uint64_t*>(S.im);
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        if (tid == 0) {
+          uint64_t all = 0;
+          for (int w = 0; w < kK3Threads / 32; ++w) all |= red[w];
+          int d = 0;
+          for (int b = 0; b < 64; b += 8) d += ((all >> b) & 0xffu) != 0;
+          atomicAdd(&P.ctl->digits[d], 1ull);
+          S.tp[1] = clock64();
+        }
+        __syncthreads();
+      }
       block_sort(S, n);
       // runs of codes equal above the slot bits, each put in (code, idx) order
       // by the thread at its first position
@@ -1609,162 +1628,6 @@ __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParam
         }
       }
     }
-  }
-}
-
-// Output pass with the survivors' records staged by the TMA.  A CTA walks the
-// fine buckets blockIdx.x, blockIdx.x + gridDim.x, ... that have survivors;
-// for each, thread 0 issues three bulk copies (cp.async.bulk, global ->
-// shared, completing on an mbarrier) of the bucket's compacted (index, re,
-// im) records into one of two stages, one bucket ahead of the stage the
-// threads are writing out from, so the record loads of bucket k+1 overlap the
-// operand gathers and output stores of bucket k.  Copies start on 16-byte
-// boundaries: every fine bucket starts on a multiple of 32 records, and a
-// copy is rounded up to 16 bytes inside the bucket's own region.  The mbarrier
-// waits are bounded: on expiry the CTA sets kFlagTimeout, waits (bounded) for
-// the copies it still has in flight and returns; the host reports
-// WG_ERR_TIMEOUT.
-constexpr int kOutThreads = 256;
-constexpr unsigned kWaitRounds = 1u << 24;  // mbarrier try_wait rounds before a copy is given up
-
-struct OutStage {
-  uint32_t idx[kCap];
-  uint64_t re[kCap];
-  double im[kCap];
-};
-struct OutSmem {
-  OutStage st[2];
-  uint64_t bar[2];
-  unsigned g[2];
-};
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-
-// Waits for the phase of `parity` to complete, at most `rounds` try_wait rounds.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned rounds) {
-  for (unsigned r = 0; r < rounds; ++r) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-template <int KW, class Src>
-__global__ void __launch_bounds__(kOutThreads) bucket_output_tma_kernel(Src src, OutputParams P) {
-  constexpr int kU = 4;
-  extern __shared__ __align__(128) unsigned char oraw[];
-  OutSmem& S = *reinterpret_cast<OutSmem*>(oraw);
-  const int tid = threadIdx.x;
-  const unsigned G = P.ctl->fine_total;
-  // the first bucket with survivors at or after g in this CTA's stride
-  auto next_bucket = [&](unsigned g) {
-    for (; g < G; g += gridDim.x)
-      if (P.counts[g]) return g;
-    return G;
-  };
-  // thread 0: the bucket's records into stage st
-  auto issue = [&](unsigned g, int st) {
-    const uint32_t cnt = P.counts[g];
-    const uint32_t start = P.fine_start[g];
-    const unsigned b4 = ((cnt + 3u) & ~3u) * 4u, b8 = ((cnt + 1u) & ~1u) * 8u;
-    // this stage's earlier reads (generic proxy) before the copies' writes (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&S.bar[st], b4 + 2u * b8);
-    bulk_copy_g2s(S.st[st].idx, P.rec_idx + start, b4, &S.bar[st]);
-    bulk_copy_g2s(S.st[st].re, P.rec_re + start, b8, &S.bar[st]);
-    bulk_copy_g2s(S.st[st].im, P.rec_im + start, b8, &S.bar[st]);
-  };
-  if (tid == 0) {
-    mbar_init(&S.bar[0], 1);
-    mbar_init(&S.bar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    const unsigned g0 = next_bucket(blockIdx.x);
-    S.g[0] = g0;
-    if (g0 < G) issue(g0, 0);
-  }
-  __syncthreads();
-  unsigned parity[2] = {0u, 0u};
-  bool inflight[2] = {S.g[0] < G, false};  // thread 0's record of issued copies (others unused)
-  int st = 0;
-  while (true) {
-    const unsigned g = S.g[st];
-    if (g >= G) break;
-    if (tid == 0) {
-      const unsigned gn = next_bucket(g + gridDim.x);
-      S.g[st ^ 1] = gn;
-      if (gn < G) {
-        issue(gn, st ^ 1);
-        inflight[st ^ 1] = true;
-      }
-    }
-    const bool ok = mbar_wait(&S.bar[st], parity[st], kWaitRounds);
-    parity[st] ^= 1u;
-    if (tid == 0) inflight[st] = false;
-    if (!__syncthreads_and(ok)) {
-      // a copy did not land: flag it, let the other stage's copy (if any) finish, stop
-      if (tid == 0) {
-        atomicOr(P.flags, kFlagTimeout);
-        if (inflight[st ^ 1]) (void)mbar_wait(&S.bar[st ^ 1], parity[st ^ 1], kWaitRounds);
-      }
-      return;
-    }
-    const uint32_t cnt = P.counts[g];
-    const size_t base = P.offsets[g];
-    if (base + cnt > P.out_cap) {
-      if (tid == 0) atomicOr(P.flags, kFlagOverrun);
-    } else {
-      const OutStage& in = S.st[st];
-      for (uint32_t i0 = tid; i0 < cnt; i0 += kOutThreads * kU) {
-        uint64_t k[kU][KW];
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const uint32_t i = i0 + kOutThreads * u;
-          if (i < cnt) src.key(in.idx[i], k[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const uint32_t i = i0 + kOutThreads * u;
-          if (i < cnt) {
-            const size_t o = base + i;
-            if (KW == 4) {
-              reinterpret_cast<ulonglong2*>(P.out_x)[o] = make_ulonglong2(k[u][0], k[u][2]);
-              reinterpret_cast<ulonglong2*>(P.out_z)[o] = make_ulonglong2(k[u][1], k[u][3]);
-            } else {
-#pragma unroll
-              for (int w = 0; w < KW / 2; ++w) {
-                P.out_x[o * (KW / 2) + w] = k[u][2 * w];
-                P.out_z[o * (KW / 2) + w] = k[u][2 * w + 1];
-              }
-            }
-            reinterpret_cast<double2*>(P.out_c)[o] =
-                make_double2(__longlong_as_double(static_cast<long long>(in.re[i])), in.im[i]);
-          }
-        }
-      }
-    }
-    __syncthreads();  // every thread is done with stage st before its next copy
-    st ^= 1;
   }
 }
 
@@ -2014,6 +1877,9 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
                  B1, h.fine_total, h.max_fine, h.refined, h.flags, U32, h.tie_items);
     std::fprintf(stderr, "bucket final phases (Gcycles, all CTAs): load %.2f sort %.2f ties %.2f sums %.2f\n",
                  h.phase[0] * 1e-9, h.phase[1] * 1e-9, h.phase[2] * 1e-9, h.phase[3] * 1e-9);
+    std::fprintf(stderr, "bucket final: fine buckets by varying code digits:");
+    for (int d = 0; d <= 8; ++d) std::fprintf(stderr, " %d:%llu", d, h.digits[d]);
+    std::fprintf(stderr, "\n");
     std::fprintf(stderr,
                  "bucket fine phases (Gcycles, all CTAs): sample %.2f splitters %.2f count %.2f scan %.2f place %.2f\n",
                  h.fphase[0] * 1e-9, h.fphase[1] * 1e-9, h.fphase[2] * 1e-9, h.fphase[3] * 1e-9, h.fphase[4] * 1e-9);
@@ -2031,10 +1897,8 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   {
     const OutputParams op{fine_start, rec_idx, rec_code, rec_im, offsets, counts, dctl,
                           ox.as<uint64_t>(), oz.as<uint64_t>(), oc.as<double>(), U, &dctl->flags};
-    auto* k4 = bucket_output_tma_kernel<KW, Src>;
-    set_smem(k4, sizeof(OutSmem));
-    const unsigned grid = static_cast<unsigned>(props.sm_count * 2);
-    WG_TIMED("bucket_output_tma_kernel", s, k4<<<grid, kOutThreads, sizeof(OutSmem), s>>>(src, op));
+    const unsigned grid = static_cast<unsigned>(props.sm_count * 8);
+    WG_TIMED("bucket_output_kernel", s, bucket_output_kernel<KW><<<grid, 256, 0, s>>>(src, op));
     wg::check_launch("launch bucket output");
   }
   unsigned flags = 0;
@@ -2042,7 +1906,6 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   wg::check_cuda(cudaStreamSynchronize(s), "synchronize bucket outputs");
   stamp("output");
   if (flags & kFlagOverrun) throw wg::Error(WG_ERR_CUDA, "bucketed simplify: output rank beyond the survivor count");
-  if (flags & kFlagTimeout) throw wg::Error(WG_ERR_TIMEOUT, "bucketed simplify: a staged record copy did not complete");
   *out.x = static_cast<uint64_t*>(ox.detach());
   *out.z = static_cast<uint64_t*>(oz.detach());
   *out.c = static_cast<double*>(oc.detach());
