@@ -1179,6 +1179,8 @@ def build_parser() -> argparse.ArgumentParser:
     ap.add_argument("--cpu-terms", type=int, default=8, help="reference terms timed for the expectation baseline")
     ap.add_argument("--ref-rows", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", choices=["off", "cached", "search"], default="cached",
+                    help="autotuner mode; a search runs in the untimed warm-up and the line records the cache")
     ap.add_argument("--sort", choices=["auto", "lsd", "bucket"], default="auto",
                     help="sort-reduce algorithm of products and simplify (results identical)")
     ap.add_argument("--lhs-terms", type=int, default=32768, help="A terms (smaller values: profiling cases)")
@@ -1217,6 +1219,10 @@ def main() -> None:
         from wolfgang_b200 import capi
 
         capi.set_sort_algorithm({"lsd": capi.WG_SORT_LSD, "bucket": capi.WG_SORT_BUCKET}[args.sort])
+    if args.autotune != "cached":
+        from wolfgang_b200 import capi
+
+        capi.autotune_mode({"off": capi.WG_TUNE_OFF, "search": capi.WG_TUNE_SEARCH}[args.autotune])
     fn = {"products": bench_products, "commutation": bench_commutation, "grouping": bench_grouping,
           "expectation": bench_expectation, "batched": bench_batched, "products_batch": bench_products_batch,
           "ops": bench_ops}[args.workload]
@@ -1225,6 +1231,10 @@ def main() -> None:
     out.update(n_gpus=world, steps=args.steps, warmup=args.warmup, scaling="weak",
                vs_baseline=None, dtype="u64" if args.workload in ("commutation", "grouping") else "f64",
                data=f"synthetic (seeded generator, workload {args.workload})")
+    if args.autotune != "cached":
+        from wolfgang_b200 import capi
+
+        out.setdefault("config", {})["autotune"] = {"mode": args.autotune, "cache": capi.autotune_export()}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
