@@ -155,6 +155,10 @@ __global__ void pbatch_count_kernel(const uint32_t* __restrict__ seg_pair, size_
 
 // ------------------------------------------------------------- numeric pass
 
+// The magnitude of a product, out of line: kMaxInf needs it only for the rare
+// product with a part beyond 2^1022 or not finite.
+__device__ __noinline__ double product_magnitude(double re, double im) { return wgd::hypot_ref(re, im); }
+
 // One thread per segment (a warp takes 32 consecutive segments): the
 // segment's products formed from the current coefficients and summed left to
 // right (FP64, no FMA: the reference's rounding); in SIMPLIFY mode the
@@ -162,10 +166,11 @@ __global__ void pbatch_count_kernel(const uint32_t* __restrict__ seg_pair, size_
 // doubles order like their bits; a NaN never replaces the running maximum,
 // std::max's rule) -- with rtol = 0 only the magnitudes that may be infinite
 // (a part beyond 2^1022 or not finite) are formed, since a finite maximum
-// leaves the threshold at atol.
+// leaves the threshold at atol.  want_max is a MaxMode.
+template <int want_max>
 __global__ void __launch_bounds__(kThreads) pbatch_sums_kernel(
     const PairNum* __restrict__ pairs, const uint32_t* __restrict__ seg_start, const uint32_t* __restrict__ seg_pair,
-    const uint32_t* __restrict__ code, size_t S, int want_max, double* __restrict__ segsum,
+    const uint32_t* __restrict__ code, size_t S, double* __restrict__ segsum,
     unsigned long long* __restrict__ pair_max) {
   const int lane = threadIdx.x & 31;
   const size_t warp = (blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5;
@@ -189,9 +194,11 @@ __global__ void __launch_bounds__(kThreads) pbatch_sums_kernel(
         const double2 bv = __ldg(reinterpret_cast<const double2*>(P.rc) + r);
         const c128 prod = wgd::rotate(wgd::cmul(c128{av.x, av.y}, c128{bv.x, bv.y}), cj & 3u);
         acc = wgd::cadd(acc, prod);
-        if (want_max == kMaxFull ||
-            (want_max == kMaxInf && !(fabs(prod.re) <= 0x1p1022 && fabs(prod.im) <= 0x1p1022))) {
+        if (want_max == kMaxFull) {
           const double m = wgd::hypot_ref(prod.re, prod.im);
+          if (mx < m) mx = m;
+        } else if (want_max == kMaxInf && !(fabs(prod.re) <= 0x1p1022 && fabs(prod.im) <= 0x1p1022)) {
+          const double m = product_magnitude(prod.re, prod.im);
           if (mx < m) mx = m;
         }
       }
@@ -409,11 +416,12 @@ void run_batch(wg_products_batch_s& b, cudaStream_t s) {
   const int max_mode = fused ? kMaxNone : b.rtol > 0.0 ? kMaxFull : kMaxInf;
   if (!fused)
     wg::check_cuda(cudaMemsetAsync(b.pair_max.get(), 0, sizeof(unsigned long long) * b.n_pairs, s), "clear maxima");
+  auto* sums = max_mode == kMaxNone ? pbatch_sums_kernel<kMaxNone>
+               : max_mode == kMaxInf ? pbatch_sums_kernel<kMaxInf> : pbatch_sums_kernel<kMaxFull>;
   WG_TIMED("pbatch_sums_kernel", s,
-    pbatch_sums_kernel<<<b.sum_blocks, kThreads, 0, s>>>(b.pairs.as<PairNum>(), b.seg_start.as<uint32_t>(),
-                                                         b.seg_pair.as<uint32_t>(), b.code.as<uint32_t>(), S,
-                                                         max_mode, b.segsum.as<double>(),
-                                                         b.pair_max.as<unsigned long long>()));
+    sums<<<b.sum_blocks, kThreads, 0, s>>>(b.pairs.as<PairNum>(), b.seg_start.as<uint32_t>(),
+                                           b.seg_pair.as<uint32_t>(), b.code.as<uint32_t>(), S,
+                                           b.segsum.as<double>(), b.pair_max.as<unsigned long long>()));
   wg::check_launch("launch batch sums");
   const unsigned g = wg::grid_for(S, kThreads, device, 8);
   WG_TIMED("pbatch_keep_kernel", s,
