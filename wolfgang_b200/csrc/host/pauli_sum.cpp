@@ -8,13 +8,16 @@
 #include "wolfgang/pauli_sum.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <bit>
 #include <cmath>
 #include <complex>
 #include <exception>
 #include <limits>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <unordered_set>
 #include <utility>
@@ -42,31 +45,69 @@ char letter(bool xb, bool zb) { return xb ? (zb ? 'Y' : 'X') : (zb ? 'Z' : 'I');
 
 // Result vectors of a large download.  A value-initialised std::vector of
 // many gigabytes spends its construction on page faults and on writing zeros
-// that the download then overwrites.  Here the storage is reserved, advised
-// for transparent huge pages and pre-faulted by several threads
-// (MADV_POPULATE_WRITE over disjoint ranges); the vectors are then filled by
-// appending the downloaded chunks (each element written once), x, z and the
-// coefficients concurrently, each through its own pinned staging.  Small
-// results take the plain path.
+// that the download then overwrites.  Here the storage is reserved and
+// advised for transparent huge pages; a pool of threads pre-faults it
+// (MADV_POPULATE_WRITE) in slices of the download's chunk size, in download
+// order across the three vectors, while x, z and the coefficients are
+// downloaded concurrently, each through its own pinned staging, and appended
+// chunk by chunk (each element written once).  A chunk's append waits only
+// for its own slice, so faulting the later slices overlaps the copies of the
+// earlier ones.  Small results take the plain path.
 constexpr std::size_t kBigHostBytes = std::size_t{64} << 20;
+constexpr std::size_t kSliceBytes = std::size_t{64} << 20;  // = the chunk size of wg_memcpy_dtoh_chunked
 
-void prefault(void* p, std::size_t bytes, unsigned threads) {
-  const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
-  const std::uintptr_t lo = (reinterpret_cast<std::uintptr_t>(p) + page - 1) & ~(page - 1);
-  const std::uintptr_t hi = (reinterpret_cast<std::uintptr_t>(p) + bytes) & ~(page - 1);
-  if (hi <= lo) return;
+// Slices [k * kSliceBytes, (k + 1) * kSliceBytes) of one vector's storage.
+struct FaultPlan {
+  char* base = nullptr;
+  std::size_t bytes = 0;
+  std::unique_ptr<std::atomic<bool>[]> done;
+  std::size_t slices() const { return (bytes + kSliceBytes - 1) / kSliceBytes; }
+  void init(void* p, std::size_t n) {
+    base = static_cast<char*>(p);
+    bytes = n;
+    done.reset(new std::atomic<bool>[slices()]);
+    for (std::size_t k = 0; k < slices(); ++k) done[k].store(false, std::memory_order_relaxed);
 #ifdef MADV_HUGEPAGE
-  madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only: failures are harmless
+    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
+    const std::uintptr_t lo = (reinterpret_cast<std::uintptr_t>(p) + page - 1) & ~(page - 1);
+    const std::uintptr_t hi = (reinterpret_cast<std::uintptr_t>(p) + n) & ~(page - 1);
+    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only
 #endif
-#ifdef MADV_POPULATE_WRITE
-  const std::size_t span = hi - lo, step = ((span / threads) + page - 1) & ~(page - 1);
-  std::vector<std::thread> pool;
-  for (std::uintptr_t a = lo; a < hi; a += step) {
-    const std::size_t len = std::min<std::size_t>(step, hi - a);
-    pool.emplace_back([a, len] { madvise(reinterpret_cast<void*>(a), len, MADV_POPULATE_WRITE); });
   }
-  for (auto& t : pool) t.join();
+  // Faults in the whole pages inside slice k (pages shared with a neighbour
+  // are faulted by the first write), then marks it done.
+  void fault(std::size_t k) {
+#ifdef MADV_POPULATE_WRITE
+    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
+    const std::uintptr_t a = reinterpret_cast<std::uintptr_t>(base) + k * kSliceBytes;
+    const std::uintptr_t e = reinterpret_cast<std::uintptr_t>(base) + std::min(bytes, (k + 1) * kSliceBytes);
+    const std::uintptr_t lo = (a + page - 1) & ~(page - 1), hi = e & ~(page - 1);
+    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
 #endif
+    done[k].store(true, std::memory_order_release);
+    done[k].notify_all();
+  }
+  void wait(std::size_t k) const {
+    while (!done[k].load(std::memory_order_acquire)) done[k].wait(false, std::memory_order_acquire);
+  }
+};
+
+// Appends the device buffer's first `count` elements to v (capacity reserved),
+// chunk k after slice k of `plan` is faulted.
+template <typename T>
+void append_after_faults(const DeviceBuffer& b, std::vector<T>& v, std::size_t count, const FaultPlan& plan) {
+  struct Ctx {
+    std::vector<T>* v;
+    const FaultPlan* plan;
+    std::size_t k;
+  } ctx{&v, &plan, 0};
+  auto fn = [](void* user, const void* chunk, std::size_t bytes) {
+    auto* c = static_cast<Ctx*>(user);
+    c->plan->wait(c->k++);
+    const T* p = static_cast<const T*>(chunk);
+    c->v->insert(c->v->end(), p, p + bytes / sizeof(T));
+  };
+  abi::check(wg_memcpy_dtoh_chunked(b.device(), b.get(), count * sizeof(T), fn, &ctx, nullptr));
 }
 
 void fetch_result_vectors(const DeviceBuffer& bx, const DeviceBuffer& bz, const DeviceBuffer& bc,
@@ -84,37 +125,49 @@ void fetch_result_vectors(const DeviceBuffer& bx, const DeviceBuffer& bz, const 
   x.reserve(words_total);
   z.reserve(words_total);
   c.reserve(terms);
-  const unsigned hw = std::max(3u, std::min(16u, std::thread::hardware_concurrency()));
-  {
-    std::thread tx([&] { prefault(x.data(), 8 * words_total, hw / 3); });
-    std::thread tz([&] { prefault(z.data(), 8 * words_total, hw / 3); });
-    prefault(c.data(), 16 * terms, hw / 3);
-    tx.join();
-    tz.join();
+  FaultPlan plans[3];
+  plans[0].init(x.data(), 8 * words_total);
+  plans[1].init(z.data(), 8 * words_total);
+  plans[2].init(c.data(), 16 * terms);
+  // fault work in download order: slice 0 of x, z, c, then slice 1, ...
+  std::atomic<std::size_t> next{0};
+  const std::size_t most = std::max(plans[0].slices(), plans[2].slices());
+  auto faulter = [&] {
+    for (std::size_t w; (w = next.fetch_add(1)) < 3 * most;) {
+      FaultPlan& pl = plans[w % 3];
+      if (w / 3 < pl.slices()) pl.fault(w / 3);
+    }
+  };
+  const unsigned hw = std::max(4u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  try {
+    for (unsigned t = 0; t + 3 < hw; ++t) pool.emplace_back(faulter);
+  } catch (const std::system_error&) {  // no threads to spare: the faulting runs here, first
   }
-  std::exception_ptr ex, ez;
+  if (pool.empty()) faulter();
+  std::exception_ptr ex, ez, ec;
   std::thread tx([&] {
     try {
-      bx.append_to(x, words_total);
+      append_after_faults(bx, x, words_total, plans[0]);
     } catch (...) {
       ex = std::current_exception();
     }
   });
   std::thread tz([&] {
     try {
-      bz.append_to(z, words_total);
+      append_after_faults(bz, z, words_total, plans[1]);
     } catch (...) {
       ez = std::current_exception();
     }
   });
-  std::exception_ptr ec;
   try {
-    bc.append_to(c, terms);
+    append_after_faults(bc, c, terms, plans[2]);
   } catch (...) {
     ec = std::current_exception();
   }
   tx.join();
   tz.join();
+  for (auto& t : pool) t.join();  // the faulters finish every slice, so no append waits forever
   for (const auto& e : {ex, ez, ec})
     if (e) std::rethrow_exception(e);
 }
