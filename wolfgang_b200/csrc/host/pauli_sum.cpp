@@ -14,7 +14,9 @@
 #include <complex>
 #include <exception>
 #include <limits>
+#include <condition_variable>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <system_error>
@@ -61,6 +63,8 @@ struct FaultPlan {
   char* base = nullptr;
   std::size_t bytes = 0;
   std::unique_ptr<std::atomic<bool>[]> done;
+  std::mutex mu;  // with cv: an append waits for its slice
+  std::condition_variable cv;
   std::size_t slices() const { return (bytes + kSliceBytes - 1) / kSliceBytes; }
   void init(void* p, std::size_t n) {
     base = static_cast<char*>(p);
@@ -84,21 +88,26 @@ struct FaultPlan {
     const std::uintptr_t lo = (a + page - 1) & ~(page - 1), hi = e & ~(page - 1);
     if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
 #endif
-    done[k].store(true, std::memory_order_release);
-    done[k].notify_all();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      done[k].store(true, std::memory_order_release);
+    }
+    cv.notify_all();
   }
-  void wait(std::size_t k) const {
-    while (!done[k].load(std::memory_order_acquire)) done[k].wait(false, std::memory_order_acquire);
+  void wait(std::size_t k) {
+    if (done[k].load(std::memory_order_acquire)) return;
+    std::unique_lock<std::mutex> lk(mu);
+    cv.wait(lk, [&] { return done[k].load(std::memory_order_acquire); });
   }
 };
 
 // Appends the device buffer's first `count` elements to v (capacity reserved),
 // chunk k after slice k of `plan` is faulted.
 template <typename T>
-void append_after_faults(const DeviceBuffer& b, std::vector<T>& v, std::size_t count, const FaultPlan& plan) {
+void append_after_faults(const DeviceBuffer& b, std::vector<T>& v, std::size_t count, FaultPlan& plan) {
   struct Ctx {
     std::vector<T>* v;
-    const FaultPlan* plan;
+    FaultPlan* plan;
     std::size_t k;
   } ctx{&v, &plan, 0};
   auto fn = [](void* user, const void* chunk, std::size_t bytes) {
