@@ -12,9 +12,11 @@
 #include <bit>
 #include <cmath>
 #include <complex>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
 #include <exception>
 #include <limits>
-#include <condition_variable>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -47,47 +49,33 @@ char letter(bool xb, bool zb) { return xb ? (zb ? 'Y' : 'X') : (zb ? 'Z' : 'I');
 
 // Result vectors of a large download.  A value-initialised std::vector of
 // many gigabytes spends its construction on page faults and on writing zeros
-// that the download then overwrites.  Here the storage is reserved and
-// advised for transparent huge pages; a pool of threads pre-faults it
-// (MADV_POPULATE_WRITE) in slices of the download's chunk size, in download
-// order across the three vectors, while x, z and the coefficients are
-// downloaded concurrently, each through its own pinned staging, and appended
-// chunk by chunk (each element written once).  A chunk's append waits only
-// for its own slice, so faulting the later slices overlaps the copies of the
-// earlier ones.  Small results take the plain path.
+// that the download then overwrites, and filling one by appending is a single
+// copy stream.  Here, per vector, the storage is reserved and advised for
+// transparent huge pages, and three stages run over slices of the download's
+// chunk size, each slice after the previous stage has finished it:
+//   fault -- a pool of threads pre-faults the slices (MADV_POPULATE_WRITE), in
+//            download order across the three vectors;
+//   size  -- one thread per vector grows the vector over the faulted slice
+//            (resize: a zero fill of pages already present);
+//   copy  -- the downloaded chunk (x, z and the coefficients are downloaded
+//            concurrently, each through its own pinned staging) is copied
+//            into the sized slice by several threads of a copy pool.
+// Each thread writes distinct elements, and the vector object itself is only
+// touched by its sizing thread; the storage never moves (the capacity is
+// reserved first).  Small results take the plain path.
 constexpr std::size_t kBigHostBytes = std::size_t{64} << 20;
 constexpr std::size_t kSliceBytes = std::size_t{64} << 20;  // = the chunk size of wg_memcpy_dtoh_chunked
 
-// Slices [k * kSliceBytes, (k + 1) * kSliceBytes) of one vector's storage.
-struct FaultPlan {
-  char* base = nullptr;
-  std::size_t bytes = 0;
+// Done flags of one stage over a vector's slices.
+struct SliceFlags {
   std::unique_ptr<std::atomic<bool>[]> done;
-  std::mutex mu;  // with cv: an append waits for its slice
+  std::mutex mu;
   std::condition_variable cv;
-  std::size_t slices() const { return (bytes + kSliceBytes - 1) / kSliceBytes; }
-  void init(void* p, std::size_t n) {
-    base = static_cast<char*>(p);
-    bytes = n;
-    done.reset(new std::atomic<bool>[slices()]);
-    for (std::size_t k = 0; k < slices(); ++k) done[k].store(false, std::memory_order_relaxed);
-#ifdef MADV_HUGEPAGE
-    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
-    const std::uintptr_t lo = (reinterpret_cast<std::uintptr_t>(p) + page - 1) & ~(page - 1);
-    const std::uintptr_t hi = (reinterpret_cast<std::uintptr_t>(p) + n) & ~(page - 1);
-    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only
-#endif
+  void init(std::size_t n) {
+    done.reset(new std::atomic<bool>[n]);
+    for (std::size_t k = 0; k < n; ++k) done[k].store(false, std::memory_order_relaxed);
   }
-  // Faults in the whole pages inside slice k (pages shared with a neighbour
-  // are faulted by the first write), then marks it done.
-  void fault(std::size_t k) {
-#ifdef MADV_POPULATE_WRITE
-    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
-    const std::uintptr_t a = reinterpret_cast<std::uintptr_t>(base) + k * kSliceBytes;
-    const std::uintptr_t e = reinterpret_cast<std::uintptr_t>(base) + std::min(bytes, (k + 1) * kSliceBytes);
-    const std::uintptr_t lo = (a + page - 1) & ~(page - 1), hi = e & ~(page - 1);
-    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
-#endif
+  void mark(std::size_t k) {
     {
       std::lock_guard<std::mutex> lk(mu);
       done[k].store(true, std::memory_order_release);
@@ -101,20 +89,141 @@ struct FaultPlan {
   }
 };
 
-// Appends the device buffer's first `count` elements to v (capacity reserved),
-// chunk k after slice k of `plan` is faulted.
+// Slices [k * kSliceBytes, (k + 1) * kSliceBytes) of one vector's storage.
+struct FaultPlan {
+  char* base = nullptr;
+  std::size_t bytes = 0;
+  SliceFlags faulted, sized;
+  std::size_t slices() const { return (bytes + kSliceBytes - 1) / kSliceBytes; }
+  void init(void* p, std::size_t n) {
+    base = static_cast<char*>(p);
+    bytes = n;
+    faulted.init(slices());
+    sized.init(slices());
+#ifdef MADV_HUGEPAGE
+    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
+    const std::uintptr_t lo = (reinterpret_cast<std::uintptr_t>(p) + page - 1) & ~(page - 1);
+    const std::uintptr_t hi = (reinterpret_cast<std::uintptr_t>(p) + n) & ~(page - 1);
+    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only
+#endif
+  }
+  // Faults in the whole pages inside slice k (pages shared with a neighbour
+  // are faulted by the first write), then marks it.
+  void fault(std::size_t k) {
+#ifdef MADV_POPULATE_WRITE
+    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
+    const std::uintptr_t a = reinterpret_cast<std::uintptr_t>(base) + k * kSliceBytes;
+    const std::uintptr_t e = reinterpret_cast<std::uintptr_t>(base) + std::min(bytes, (k + 1) * kSliceBytes);
+    const std::uintptr_t lo = (a + page - 1) & ~(page - 1), hi = e & ~(page - 1);
+    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
+#endif
+    faulted.mark(k);
+  }
+};
+
+// Worker threads that copy pieces of chunks; a copy call returns once all of
+// its pieces are done.  Without workers the caller copies alone.
+class CopyPool {
+ public:
+  explicit CopyPool(unsigned n) {
+    try {
+      for (unsigned t = 0; t < n; ++t) workers_.emplace_back([this] { work(); });
+    } catch (const std::system_error&) {  // fewer workers
+    }
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  void copy(void* dst, const void* src, std::size_t bytes) {
+    constexpr std::size_t kPiece = std::size_t{8} << 20;
+    const std::size_t pieces = (bytes + kPiece - 1) / kPiece;
+    if (workers_.empty() || pieces < 2) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    Done done;
+    done.left = pieces - 1;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (std::size_t q = 1; q < pieces; ++q)
+        tasks_.push_back(Task{static_cast<char*>(dst) + q * kPiece, static_cast<const char*>(src) + q * kPiece,
+                              std::min(kPiece, bytes - q * kPiece), &done});
+    }
+    cv_.notify_all();
+    std::memcpy(dst, src, std::min(kPiece, bytes));  // the first piece, here
+    std::unique_lock<std::mutex> lk(done.mu);
+    done.cv.wait(lk, [&] { return done.left == 0; });
+  }
+
+ private:
+  struct Done {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::size_t left = 0;
+  };
+  struct Task {
+    char* dst;
+    const char* src;
+    std::size_t bytes;
+    Done* done;
+  };
+  void work() {
+    for (;;) {
+      Task t;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+        if (tasks_.empty()) return;
+        t = tasks_.front();
+        tasks_.pop_front();
+      }
+      std::memcpy(t.dst, t.src, t.bytes);
+      {
+        std::lock_guard<std::mutex> lk(t.done->mu);
+        --t.done->left;
+      }
+      t.done->cv.notify_all();
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::deque<Task> tasks_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  bool stop_ = false;
+};
+
+// Grows v (capacity reserved) to `count` elements, one faulted slice at a time.
 template <typename T>
-void append_after_faults(const DeviceBuffer& b, std::vector<T>& v, std::size_t count, FaultPlan& plan) {
+void size_by_slices(std::vector<T>& v, std::size_t count, FaultPlan& plan) {
+  const std::size_t per = kSliceBytes / sizeof(T);
+  for (std::size_t k = 0; k < plan.slices(); ++k) {
+    plan.faulted.wait(k);
+    v.resize(std::min(count, (k + 1) * per));
+    plan.sized.mark(k);
+  }
+}
+
+// Downloads the device buffer's first `count` elements into base (the reserved
+// storage of a vector being sized by size_by_slices): chunk k is copied once
+// slice k is sized.
+template <typename T>
+void download_into_slices(const DeviceBuffer& b, T* base, std::size_t count, FaultPlan& plan, CopyPool& pool) {
   struct Ctx {
-    std::vector<T>* v;
+    char* base;
     FaultPlan* plan;
+    CopyPool* pool;
     std::size_t k;
-  } ctx{&v, &plan, 0};
+  } ctx{reinterpret_cast<char*>(base), &plan, &pool, 0};
   auto fn = [](void* user, const void* chunk, std::size_t bytes) {
     auto* c = static_cast<Ctx*>(user);
-    c->plan->wait(c->k++);
-    const T* p = static_cast<const T*>(chunk);
-    c->v->insert(c->v->end(), p, p + bytes / sizeof(T));
+    const std::size_t k = c->k++;
+    c->plan->sized.wait(k);
+    c->pool->copy(c->base + k * kSliceBytes, chunk, bytes);
   };
   abi::check(wg_memcpy_dtoh_chunked(b.device(), b.get(), count * sizeof(T), fn, &ctx, nullptr));
 }
@@ -138,6 +247,12 @@ void fetch_result_vectors(const DeviceBuffer& bx, const DeviceBuffer& bz, const 
   plans[0].init(x.data(), 8 * words_total);
   plans[1].init(z.data(), 8 * words_total);
   plans[2].init(c.data(), 16 * terms);
+  // the storage, taken before any thread resizes a vector (it never moves)
+  std::uint64_t* const xs = x.data();
+  std::uint64_t* const zs = z.data();
+  std::complex<double>* const cs = c.data();
+  const unsigned hw = std::max(4u, std::min(32u, std::thread::hardware_concurrency()));
+  CopyPool pool(hw > 6 ? hw - 6 : 1);  // besides the three download and three sizing threads
   // fault work in download order: slice 0 of x, z, c, then slice 1, ...
   std::atomic<std::size_t> next{0};
   const std::size_t most = std::max(plans[0].slices(), plans[2].slices());
@@ -147,36 +262,42 @@ void fetch_result_vectors(const DeviceBuffer& bx, const DeviceBuffer& bz, const 
       if (w / 3 < pl.slices()) pl.fault(w / 3);
     }
   };
-  const unsigned hw = std::max(4u, std::min(32u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> pool;
+  std::vector<std::thread> faulters;
   try {
-    for (unsigned t = 0; t + 3 < hw; ++t) pool.emplace_back(faulter);
+    for (unsigned t = 0; t + 3 < hw; ++t) faulters.emplace_back(faulter);
   } catch (const std::system_error&) {  // no threads to spare: the faulting runs here, first
   }
-  if (pool.empty()) faulter();
+  if (faulters.empty()) faulter();
+  std::thread sx([&] { size_by_slices(x, words_total, plans[0]); });
+  std::thread sz([&] { size_by_slices(z, words_total, plans[1]); });
+  std::thread sc([&] { size_by_slices(c, terms, plans[2]); });
   std::exception_ptr ex, ez, ec;
   std::thread tx([&] {
     try {
-      append_after_faults(bx, x, words_total, plans[0]);
+      download_into_slices(bx, xs, words_total, plans[0], pool);
     } catch (...) {
       ex = std::current_exception();
     }
   });
   std::thread tz([&] {
     try {
-      append_after_faults(bz, z, words_total, plans[1]);
+      download_into_slices(bz, zs, words_total, plans[1], pool);
     } catch (...) {
       ez = std::current_exception();
     }
   });
   try {
-    append_after_faults(bc, c, terms, plans[2]);
+    download_into_slices(bc, cs, terms, plans[2], pool);
   } catch (...) {
     ec = std::current_exception();
   }
   tx.join();
   tz.join();
-  for (auto& t : pool) t.join();  // the faulters finish every slice, so no append waits forever
+  // every slice is faulted and sized whatever the downloads did, so these end
+  sx.join();
+  sz.join();
+  sc.join();
+  for (auto& t : faulters) t.join();
   for (const auto& e : {ex, ez, ec})
     if (e) std::rethrow_exception(e);
 }
