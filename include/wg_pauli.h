@@ -91,8 +91,9 @@ int wg_memcpy_dtoh(int device, void* dst, const void* src, size_t bytes, wg_stre
 int wg_memcpy_dtod(int device, void* dst, const void* src, size_t bytes, wg_stream_t stream);
 /* Device-to-host copy delivered in chunks: the buffer goes through pinned
  * staging and each chunk is handed, in order, to fn(user, chunk, chunk_bytes)
- * on the calling thread once it has landed (chunks are 64 MiB, the last one
- * shorter).  Lets a caller build its own host container from the data without
+ * on the calling thread once it has landed (chunks are 8 MiB, the last one
+ * shorter; a ring of three pinned buffers per call keeps two chunks in flight
+ * while the caller consumes one).  Lets a caller build its own host container from the data without
  * first filling it (e.g. appending to a reserved std::vector).  Calls from
  * different threads run concurrently, each with its own staging and stream.
  * Ordering: the copies run on an internal stream that first waits for all

@@ -413,13 +413,14 @@ def test_device_errors():
 @pytest.mark.parametrize("simplify", [True, False])
 def test_large_host_result_through_public_matmul(oracle, simplify):
     """A host result above 64 MB takes the large-result path (storage reserved,
-    faulted, sized and filled slice by slice while the chunks are downloaded):
-    the public PauliSum.matmul result equals the oracle bit for bit."""
+    each vector grown by appending the downloaded chunks piece by piece behind
+    fault-ahead helpers): the public PauliSum.matmul result equals the oracle
+    bit for bit."""
     from wolfgang_b200.workloads import klocal_operator
 
     rng = np.random.default_rng(640)
     A = klocal_operator(rng, 100, 4096, np.array([2, 3, 4]))
-    B = klocal_operator(rng, 100, 2300, np.array([2, 3, 4]))  # 9.4e6 products: each vector spans 3 slices
+    B = klocal_operator(rng, 100, 2300, np.array([2, 3, 4]))  # 9.4e6 products: each vector spans many 2 MiB pieces and 8 MiB chunks
     hA = PauliSum._from_packed(100, A[1], A[2], A[3])
     hB = PauliSum._from_packed(100, B[1], B[2], B[3])
     x, z, c = hA.matmul(hB, simplify=simplify, max_intermediate_terms=len(A[3]) * len(B[3]))._packed()

@@ -262,8 +262,8 @@ def test_sort_algorithm_rejects_unknown(cuda):
 @pytest.mark.parametrize("nl,nr", [(2048, 1024), (4096, 2048)])
 def test_public_matmul_large_host_result(cuda, algo, nl, nr):
     """PauliSum.matmul through the public API with a host result above 64 MiB
-    (pre-faulted result vectors filled by appending the downloaded chunks; the
-    larger case spans several 64 MiB chunks per vector) equals the device-side
+    (result vectors grown by appending the downloaded chunks behind fault-ahead
+    helpers; the larger case spans many 8 MiB chunks per vector) equals the device-side
     products of the C-ABI, downloaded directly."""
     import wolfgang_quantum as wq
 

@@ -10,11 +10,13 @@
 #include <algorithm>
 #include <atomic>
 #include <bit>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
-#include <deque>
 #include <exception>
 #include <limits>
 #include <memory>
@@ -49,181 +51,136 @@ char letter(bool xb, bool zb) { return xb ? (zb ? 'Y' : 'X') : (zb ? 'Z' : 'I');
 
 // Result vectors of a large download.  A value-initialised std::vector of
 // many gigabytes spends its construction on page faults and on writing zeros
-// that the download then overwrites, and filling one by appending is a single
-// copy stream.  Here, per vector, the storage is reserved and advised for
-// transparent huge pages, and three stages run over slices of the download's
-// chunk size, each slice after the previous stage has finished it:
-//   fault -- a pool of threads pre-faults the slices (MADV_POPULATE_WRITE), in
-//            download order across the three vectors;
-//   size  -- one thread per vector grows the vector over the faulted slice
-//            (resize: a zero fill of pages already present);
-//   copy  -- the downloaded chunk (x, z and the coefficients are downloaded
-//            concurrently, each through its own pinned staging) is copied
-//            into the sized slice by several threads of a copy pool.
-// Each thread writes distinct elements, and the vector object itself is only
-// touched by its sizing thread; the storage never moves (the capacity is
-// reserved first).  Small results take the plain path.
+// that the download then overwrites.  Here each vector's storage is reserved
+// and advised for transparent huge pages, and the vector grows by appending
+// the downloaded chunks (x, z and the coefficients download concurrently,
+// each through its own pinned staging, and each download thread appends to
+// its own vector).  The appends go piece by piece over a grid of 2 MiB
+// aligned pieces, and helper threads fault in (MADV_POPULATE_WRITE) the
+// pieces a short distance ahead of the append: the kernel's zero fill of a
+// page and the append's stores then meet the same lines while they are still
+// in the caches, instead of each writing the page to memory.  The vector
+// object is only touched by its download thread; the helpers touch pages of
+// the reserved storage, which never moves.  Small results take the plain path.
 constexpr std::size_t kBigHostBytes = std::size_t{64} << 20;
-constexpr std::size_t kSliceBytes = std::size_t{64} << 20;  // = the chunk size of wg_memcpy_dtoh_chunked
+constexpr std::size_t kPieceBytes = std::size_t{2} << 20;
+constexpr std::size_t kFaultAhead = 2;  // pieces a helper may fault beyond the append
 
-// Done flags of one stage over a vector's slices.
-struct SliceFlags {
-  std::unique_ptr<std::atomic<bool>[]> done;
-  std::mutex mu;
-  std::condition_variable cv;
-  void init(std::size_t n) {
-    done.reset(new std::atomic<bool>[n]);
-    for (std::size_t k = 0; k < n; ++k) done[k].store(false, std::memory_order_relaxed);
-  }
-  void mark(std::size_t k) {
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      done[k].store(true, std::memory_order_release);
-    }
-    cv.notify_all();
-  }
-  void wait(std::size_t k) {
-    if (done[k].load(std::memory_order_acquire)) return;
-    std::unique_lock<std::mutex> lk(mu);
-    cv.wait(lk, [&] { return done[k].load(std::memory_order_acquire); });
-  }
-};
-
-// Slices [k * kSliceBytes, (k + 1) * kSliceBytes) of one vector's storage.
-struct FaultPlan {
-  char* base = nullptr;
-  std::size_t bytes = 0;
-  SliceFlags faulted, sized;
-  std::size_t slices() const { return (bytes + kSliceBytes - 1) / kSliceBytes; }
-  void init(void* p, std::size_t n) {
-    base = static_cast<char*>(p);
-    bytes = n;
-    faulted.init(slices());
-    sized.init(slices());
+// Faults in the pieces of [base, base + bytes) ahead of an append.
+class FaultAhead {
+ public:
+  FaultAhead(void* base, std::size_t bytes, unsigned threads)
+      : base_(reinterpret_cast<std::uintptr_t>(base)),
+        bytes_(bytes),
+        grid_(base_ & ~std::uintptr_t{kPieceBytes - 1}),
+        pieces_((base_ + bytes - grid_ + kPieceBytes - 1) / kPieceBytes),
+        faulted_(new bool[pieces_]()) {
 #ifdef MADV_HUGEPAGE
-    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
-    const std::uintptr_t lo = (reinterpret_cast<std::uintptr_t>(p) + page - 1) & ~(page - 1);
-    const std::uintptr_t hi = (reinterpret_cast<std::uintptr_t>(p) + n) & ~(page - 1);
+    const std::uintptr_t lo = round_up(base_), hi = round_down(base_ + bytes_);
     if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_HUGEPAGE);  // advice only
 #endif
-  }
-  // Faults in the whole pages inside slice k (pages shared with a neighbour
-  // are faulted by the first write), then marks it.
-  void fault(std::size_t k) {
 #ifdef MADV_POPULATE_WRITE
-    const std::size_t page = static_cast<std::size_t>(sysconf(_SC_PAGESIZE));
-    const std::uintptr_t a = reinterpret_cast<std::uintptr_t>(base) + k * kSliceBytes;
-    const std::uintptr_t e = reinterpret_cast<std::uintptr_t>(base) + std::min(bytes, (k + 1) * kSliceBytes);
-    const std::uintptr_t lo = (a + page - 1) & ~(page - 1), hi = e & ~(page - 1);
-    if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
-#endif
-    faulted.mark(k);
-  }
-};
-
-// Worker threads that copy pieces of chunks; a copy call returns once all of
-// its pieces are done.  Without workers the caller copies alone.
-class CopyPool {
- public:
-  explicit CopyPool(unsigned n) {
     try {
-      for (unsigned t = 0; t < n; ++t) workers_.emplace_back([this] { work(); });
-    } catch (const std::system_error&) {  // fewer workers
+      for (unsigned t = 0; t < threads; ++t) helpers_.emplace_back([this] { work(); });
+    } catch (const std::system_error&) {  // fewer helpers: the appends fault what is left
     }
+#else
+    (void)threads;
+#endif
   }
-  ~CopyPool() {
+  ~FaultAhead() {
     {
       std::lock_guard<std::mutex> lk(mu_);
       stop_ = true;
     }
     cv_.notify_all();
-    for (auto& t : workers_) t.join();
+    for (auto& t : helpers_) t.join();
   }
-  void copy(void* dst, const void* src, std::size_t bytes) {
-    constexpr std::size_t kPiece = std::size_t{8} << 20;
-    const std::size_t pieces = (bytes + kPiece - 1) / kPiece;
-    if (workers_.empty() || pieces < 2) {
-      std::memcpy(dst, src, bytes);
-      return;
-    }
-    Done done;
-    done.left = pieces - 1;
+  FaultAhead(const FaultAhead&) = delete;
+  FaultAhead& operator=(const FaultAhead&) = delete;
+
+  // Byte offsets from base where piece k starts and ends (base is 16-byte
+  // aligned, so every piece holds whole elements).
+  std::size_t start(std::size_t k) const { return k == 0 ? 0 : grid_ + k * kPieceBytes - base_; }
+  std::size_t end(std::size_t k) const { return k + 1 < pieces_ ? start(k + 1) : bytes_; }
+  std::size_t piece_of(std::size_t off) const { return (base_ + off - grid_) / kPieceBytes; }
+
+  // Waits until piece k is faulted in (at once when no helper runs).
+  void wait(std::size_t k) {
+    if (helpers_.empty()) return;
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return faulted_[k]; });
+  }
+  // The append has filled pieces [0, k]: helpers may fault up to k + 1 + kFaultAhead.
+  void appended(std::size_t k) {
     {
       std::lock_guard<std::mutex> lk(mu_);
-      for (std::size_t q = 1; q < pieces; ++q)
-        tasks_.push_back(Task{static_cast<char*>(dst) + q * kPiece, static_cast<const char*>(src) + q * kPiece,
-                              std::min(kPiece, bytes - q * kPiece), &done});
+      appended_ = k + 1;
     }
     cv_.notify_all();
-    std::memcpy(dst, src, std::min(kPiece, bytes));  // the first piece, here
-    std::unique_lock<std::mutex> lk(done.mu);
-    done.cv.wait(lk, [&] { return done.left == 0; });
   }
 
  private:
-  struct Done {
-    std::mutex mu;
-    std::condition_variable cv;
-    std::size_t left = 0;
-  };
-  struct Task {
-    char* dst;
-    const char* src;
-    std::size_t bytes;
-    Done* done;
-  };
+  static std::uintptr_t page() { return static_cast<std::uintptr_t>(sysconf(_SC_PAGESIZE)); }
+  static std::uintptr_t round_up(std::uintptr_t a) { return (a + page() - 1) & ~(page() - 1); }
+  static std::uintptr_t round_down(std::uintptr_t a) { return a & ~(page() - 1); }
   void work() {
     for (;;) {
-      Task t;
+      const std::size_t k = next_.fetch_add(1);
+      if (k >= pieces_) return;
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
-        if (tasks_.empty()) return;
-        t = tasks_.front();
-        tasks_.pop_front();
+        cv_.wait(lk, [&] { return stop_ || k <= appended_ + kFaultAhead; });
+        if (stop_) return;
       }
-      std::memcpy(t.dst, t.src, t.bytes);
+#ifdef MADV_POPULATE_WRITE
+      // whole pages inside the piece; a page shared with a neighbour piece
+      // (only at the ends of the storage) is faulted by the first write
+      const std::uintptr_t lo = round_up(base_ + start(k)), hi = round_down(base_ + end(k));
+      if (hi > lo) madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
+#endif
       {
-        std::lock_guard<std::mutex> lk(t.done->mu);
-        --t.done->left;
+        std::lock_guard<std::mutex> lk(mu_);
+        faulted_[k] = true;
       }
-      t.done->cv.notify_all();
+      cv_.notify_all();
     }
   }
-  std::vector<std::thread> workers_;
-  std::deque<Task> tasks_;
+  const std::uintptr_t base_;
+  const std::size_t bytes_;
+  const std::uintptr_t grid_;  // base rounded down to the piece grid
+  const std::size_t pieces_;
+  std::unique_ptr<bool[]> faulted_;
+  std::size_t appended_ = 0;  // pieces [0, appended_) are filled
+  std::atomic<std::size_t> next_{0};
+  bool stop_ = false;
   std::mutex mu_;
   std::condition_variable cv_;
-  bool stop_ = false;
+  std::vector<std::thread> helpers_;
 };
 
-// Grows v (capacity reserved) to `count` elements, one faulted slice at a time.
+// Downloads the device buffer's first `count` elements and appends them to v
+// (capacity reserved, empty), piece by piece behind the fault-ahead helpers.
 template <typename T>
-void size_by_slices(std::vector<T>& v, std::size_t count, FaultPlan& plan) {
-  const std::size_t per = kSliceBytes / sizeof(T);
-  for (std::size_t k = 0; k < plan.slices(); ++k) {
-    plan.faulted.wait(k);
-    v.resize(std::min(count, (k + 1) * per));
-    plan.sized.mark(k);
-  }
-}
-
-// Downloads the device buffer's first `count` elements into base (the reserved
-// storage of a vector being sized by size_by_slices): chunk k is copied once
-// slice k is sized.
-template <typename T>
-void download_into_slices(const DeviceBuffer& b, T* base, std::size_t count, FaultPlan& plan, CopyPool& pool) {
+void download_appending(const DeviceBuffer& b, std::vector<T>& v, std::size_t count, FaultAhead& ahead) {
   struct Ctx {
-    char* base;
-    FaultPlan* plan;
-    CopyPool* pool;
-    std::size_t k;
-  } ctx{reinterpret_cast<char*>(base), &plan, &pool, 0};
+    std::vector<T>* v;
+    FaultAhead* ahead;
+    std::size_t off;  // bytes appended so far
+  } ctx{&v, &ahead, 0};
   auto fn = [](void* user, const void* chunk, std::size_t bytes) {
     auto* c = static_cast<Ctx*>(user);
-    const std::size_t k = c->k++;
-    c->plan->sized.wait(k);
-    c->pool->copy(c->base + k * kSliceBytes, chunk, bytes);
+    const char* src = static_cast<const char*>(chunk);
+    for (std::size_t done = 0; done < bytes;) {
+      const std::size_t k = c->ahead->piece_of(c->off);
+      const std::size_t n = std::min(bytes - done, c->ahead->end(k) - c->off);
+      c->ahead->wait(k);
+      const T* s = reinterpret_cast<const T*>(src + done);
+      c->v->insert(c->v->end(), s, s + n / sizeof(T));
+      done += n;
+      c->off += n;
+      if (c->off == c->ahead->end(k)) c->ahead->appended(k);
+    }
   };
   abi::check(wg_memcpy_dtoh_chunked(b.device(), b.get(), count * sizeof(T), fn, &ctx, nullptr));
 }
@@ -240,64 +197,61 @@ void fetch_result_vectors(const DeviceBuffer& bx, const DeviceBuffer& bz, const 
     bc.download(c.data(), c.size() * 16);
     return;
   }
+  // WG_HOST_TRACE set: when each vector is filled, on stderr
+  const bool trace = std::getenv("WG_HOST_TRACE") != nullptr;
+  const auto t0 = std::chrono::steady_clock::now();
+  auto ms = [&] { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
+  double t_filled[3] = {0.0, 0.0, 0.0};
+  x.clear();
+  z.clear();
+  c.clear();
   x.reserve(words_total);
   z.reserve(words_total);
   c.reserve(terms);
-  FaultPlan plans[3];
-  plans[0].init(x.data(), 8 * words_total);
-  plans[1].init(z.data(), 8 * words_total);
-  plans[2].init(c.data(), 16 * terms);
-  // the storage, taken before any thread resizes a vector (it never moves)
-  std::uint64_t* const xs = x.data();
-  std::uint64_t* const zs = z.data();
-  std::complex<double>* const cs = c.data();
-  const unsigned hw = std::max(4u, std::min(32u, std::thread::hardware_concurrency()));
-  CopyPool pool(hw > 6 ? hw - 6 : 1);  // besides the three download and three sizing threads
-  // fault work in download order: slice 0 of x, z, c, then slice 1, ...
-  std::atomic<std::size_t> next{0};
-  const std::size_t most = std::max(plans[0].slices(), plans[2].slices());
-  auto faulter = [&] {
-    for (std::size_t w; (w = next.fetch_add(1)) < 3 * most;) {
-      FaultPlan& pl = plans[w % 3];
-      if (w / 3 < pl.slices()) pl.fault(w / 3);
-    }
-  };
-  std::vector<std::thread> faulters;
-  try {
-    for (unsigned t = 0; t + 3 < hw; ++t) faulters.emplace_back(faulter);
-  } catch (const std::system_error&) {  // no threads to spare: the faulting runs here, first
+  auto aligned16 = [](const void* p) { return reinterpret_cast<std::uintptr_t>(p) % 16 == 0; };
+  if (!aligned16(x.data()) || !aligned16(z.data()) || !aligned16(c.data())) {  // not from this allocator
+    x.resize(words_total);
+    z.resize(words_total);
+    c.resize(terms);
+    bx.download(x.data(), x.size() * 8);
+    bz.download(z.data(), z.size() * 8);
+    bc.download(c.data(), c.size() * 16);
+    return;
   }
-  if (faulters.empty()) faulter();
-  std::thread sx([&] { size_by_slices(x, words_total, plans[0]); });
-  std::thread sz([&] { size_by_slices(z, words_total, plans[1]); });
-  std::thread sc([&] { size_by_slices(c, terms, plans[2]); });
+  // two helpers per vector where the host has the threads (a helper faults at
+  // about half the rate an append consumes pages)
+  const unsigned helpers = std::thread::hardware_concurrency() >= 9 ? 2 : 1;
+  FaultAhead ax(x.data(), 8 * words_total, helpers);
+  FaultAhead az(z.data(), 8 * words_total, helpers);
+  FaultAhead ac(c.data(), 16 * terms, helpers);
   std::exception_ptr ex, ez, ec;
   std::thread tx([&] {
     try {
-      download_into_slices(bx, xs, words_total, plans[0], pool);
+      download_appending(bx, x, words_total, ax);
+      t_filled[0] = ms();
     } catch (...) {
       ex = std::current_exception();
     }
   });
   std::thread tz([&] {
     try {
-      download_into_slices(bz, zs, words_total, plans[1], pool);
+      download_appending(bz, z, words_total, az);
+      t_filled[1] = ms();
     } catch (...) {
       ez = std::current_exception();
     }
   });
   try {
-    download_into_slices(bc, cs, terms, plans[2], pool);
+    download_appending(bc, c, terms, ac);
+    t_filled[2] = ms();
   } catch (...) {
     ec = std::current_exception();
   }
   tx.join();
   tz.join();
-  // every slice is faulted and sized whatever the downloads did, so these end
-  sx.join();
-  sz.join();
-  sc.join();
-  for (auto& t : faulters) t.join();
+  if (trace)
+    std::fprintf(stderr, "host result %.2f GB: x %.1f ms, z %.1f ms, coefficients %.1f ms\n",
+                 (16.0 * words_total + 16.0 * terms) * 1e-9, t_filled[0], t_filled[1], t_filled[2]);
   for (const auto& e : {ex, ez, ec})
     if (e) std::rethrow_exception(e);
 }

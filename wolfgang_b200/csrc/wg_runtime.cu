@@ -167,11 +167,14 @@ void parallel_memcpy(char* dst, const char* src, size_t bytes) {
   std::memcpy(dst, src, std::min(part, bytes));
   for (auto& t : th) t.join();
 }
-// Staging for chunked downloads: one pair of pinned buffers, two events and a
-// stream per concurrent call, kept for reuse.
+// Staging for chunked downloads: a ring of small pinned buffers, their events
+// and a stream per concurrent call, kept for reuse.  The chunks are small and
+// the ring shallow so that a chunk is consumed soon after its DMA lands.
+constexpr size_t kChunkBytes = size_t{8} << 20;
+constexpr int kChunkRing = 3;
 struct ChunkStage {
-  void* buf[2] = {nullptr, nullptr};
-  cudaEvent_t done[2] = {nullptr, nullptr};
+  void* buf[kChunkRing] = {};
+  cudaEvent_t done[kChunkRing] = {};
   cudaEvent_t ready = nullptr;  // recorded on the caller's stream: src is complete
   cudaStream_t stream = nullptr;
   int device = -1;
@@ -193,14 +196,14 @@ ChunkStage* take_chunk_stage(int device) {
   auto* c = new ChunkStage;
   c->device = device;
   try {
-    for (int i = 0; i < 2; ++i) {
-      check_cuda(cudaHostAlloc(&c->buf[i], kStageBytes, cudaHostAllocPortable), "allocate pinned staging");
+    for (int i = 0; i < kChunkRing; ++i) {
+      check_cuda(cudaHostAlloc(&c->buf[i], kChunkBytes, cudaHostAllocPortable), "allocate pinned staging");
       check_cuda(cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming), "create staging event");
     }
     check_cuda(cudaEventCreateWithFlags(&c->ready, cudaEventDisableTiming), "create staging event");
     check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "create staging stream");
   } catch (...) {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kChunkRing; ++i) {
       if (c->buf[i]) (void)cudaFreeHost(c->buf[i]);
       if (c->done[i]) (void)cudaEventDestroy(c->done[i]);
     }
@@ -220,26 +223,27 @@ void give_chunk_stage(ChunkStage* c) {
 void chunked_download(int device, const void* src, size_t bytes, wg_chunk_fn fn, void* user, cudaStream_t after) {
   ChunkStage* c = take_chunk_stage(device);
   const char* const sp = static_cast<const char*>(src);
-  const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
-  auto len_of = [&](size_t k) { return std::min(kStageBytes, bytes - k * kStageBytes); };
+  const size_t chunks = (bytes + kChunkBytes - 1) / kChunkBytes;
+  auto len_of = [&](size_t k) { return std::min(kChunkBytes, bytes - k * kChunkBytes); };
+  constexpr size_t ahead = kChunkRing - 1;  // chunks in flight while the caller consumes one
   try {
     // The staging stream is a non-blocking stream of its own: order its copies
     // after everything already enqueued on the caller's stream (the work that
     // writes src), or they could read src before that work has finished.
     check_cuda(cudaEventRecord(c->ready, after), "record download order");
     check_cuda(cudaStreamWaitEvent(c->stream, c->ready, 0), "order download after the caller's stream");
-    // DMA chunk k into buffer k%2 while the caller consumes chunk k-1
-    for (size_t k = 0; k <= chunks; ++k) {
+    // DMA chunk k into ring buffer k % kChunkRing while the caller consumes chunk k - ahead
+    for (size_t k = 0; k < chunks + ahead; ++k) {
       if (k < chunks) {
-        check_cuda(cudaMemcpyAsync(c->buf[k & 1], sp + k * kStageBytes, len_of(k), cudaMemcpyDeviceToHost,
-                                   c->stream),
+        check_cuda(cudaMemcpyAsync(c->buf[k % kChunkRing], sp + k * kChunkBytes, len_of(k),
+                                   cudaMemcpyDeviceToHost, c->stream),
                    "copy device buffer to staging");
-        check_cuda(cudaEventRecord(c->done[k & 1], c->stream), "record staging event");
+        check_cuda(cudaEventRecord(c->done[k % kChunkRing], c->stream), "record staging event");
       }
-      if (k > 0) {
-        const size_t j = k - 1;
-        check_cuda(cudaEventSynchronize(c->done[j & 1]), "wait for staging");
-        fn(user, c->buf[j & 1], len_of(j));
+      if (k >= ahead) {
+        const size_t j = k - ahead;
+        check_cuda(cudaEventSynchronize(c->done[j % kChunkRing]), "wait for staging");
+        fn(user, c->buf[j % kChunkRing], len_of(j));
       }
     }
   } catch (...) {
