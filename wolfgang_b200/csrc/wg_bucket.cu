@@ -1446,26 +1446,25 @@ __global__ void __launch_bounds__(kK3Threads, kK3PerSM) bucket_final_kernel(Src 
       }
       __syncthreads();
       if (P.trace && tid == 0) S.tp[2] = clock64();
-      // segment heads where the code changes
+      // segment heads where the code changes, and (inexact codes) runs of
+      // equal position code, listed by the thread at the run's first position
+      // and resolved once every thread is done reading codes
       for (int i0 = warp * 32; i0 < n; i0 += kK3Threads) {
         const int i = i0 + lane;
-        const bool h = i < n && (i == 0 || S.code[pidx(i)] != S.code[pidx(i - 1)]);
+        const uint64_t ci = i < n ? S.code[pidx(i)] : 0;
+        const bool h = i < n && (i == 0 || S.code[pidx(i - 1)] != ci);
         const uint32_t b = __ballot_sync(0xffffffffu, h);
         if (lane == 0) S.head[i0 >> 5] = b;
-      }
-      if (!exact) {
-        // runs of equal position code, listed by the thread at the run's first
-        // position, then resolved once every thread is done reading codes
-        for (int i = tid; i + 1 < n; i += kK3Threads) {
-          const uint64_t ci = S.code[pidx(i)];
-          // a code with an empty eighth digit holds every set bit: one key
-          if ((ci & 0xffu) == 0 || (i > 0 && S.code[pidx(i - 1)] == ci) || S.code[pidx(i + 1)] != ci) continue;
+        // a code with an empty eighth digit holds every set bit: one key
+        if (!exact && h && i + 1 < n && (ci & 0xffu) != 0 && S.code[pidx(i + 1)] == ci) {
           int e = i + 2;
           while (e < n && S.code[pidx(e)] == ci) ++e;
           const unsigned q = atomicAdd(&S.n_runs, 1u);
           S.runs[q] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(e);
           if (P.trace) atomicAdd(&P.ctl->tie_items, static_cast<unsigned long long>(e - i));
         }
+      }
+      if (!exact) {
         __syncthreads();
         const int L = P.fine_L[g];
         const int nr = static_cast<int>(S.n_runs);
