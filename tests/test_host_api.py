@@ -139,6 +139,22 @@ def test_packed_round_trip():
         PauliSum._from_packed(3, np.array([[8]], np.uint64), np.array([[0]], np.uint64), np.ones(1))
 
 
+def test_public_packed_constructor_and_export():
+    """from_packed / to_packed: the public forms of the packed constructor and
+    export; they equal the label path and round-trip the storage exactly."""
+    labels = [label_for(130, {0: "X", 64: "Y", 129: "Z"}), label_for(130, {5: "Z", 77: "X"}), "I" * 130]
+    coeffs = [1 + 2j, -0.5, 3j]
+    op = PauliSum.from_labels(labels, coeffs)
+    x, z, c = op.to_packed()
+    assert x.shape == (3, 3) and z.shape == (3, 3) and c.dtype == np.complex128
+    back = PauliSum.from_packed(130, x, z, c)
+    assert back.to_labels()[0] == op.to_labels()[0] == labels
+    for a, b in zip(back.to_packed(), op.to_packed()):
+        assert a.tobytes() == b.tobytes()
+    with pytest.raises(ValueError, match="above num_qubits"):
+        PauliSum.from_packed(3, np.array([[8]], np.uint64), np.array([[0]], np.uint64), np.ones(1))
+
+
 def test_no_device_is_reported_as_runtime_error():
     import wolfgang_quantum as wq
 

@@ -403,6 +403,29 @@ py::object matrix_dlpack(py::object self, py::object stream, py::object max_vers
 
 }  // namespace
 
+// PauliSum from packed words (numpy arrays, converted to the storage types).
+PauliSum from_packed(long long n, py::array_t<std::uint64_t, py::array::c_style | py::array::forcecast> x,
+                     py::array_t<std::uint64_t, py::array::c_style | py::array::forcecast> z,
+                     py::array_t<std::complex<double>, py::array::c_style | py::array::forcecast> c) {
+  std::vector<std::uint64_t> vx(x.data(), x.data() + x.size()), vz(z.data(), z.data() + z.size());
+  std::vector<std::complex<double>> vc(c.data(), c.data() + c.size());
+  return translate([&] {
+    return PauliSum::from_packed(nonneg(n, "num_qubits"), std::move(vx), std::move(vz), std::move(vc));
+  });
+}
+
+// (x, z, coeffs) copies of a PauliSum's storage as numpy arrays.
+py::tuple to_packed(const PauliSum& p) {
+  const auto T = static_cast<py::ssize_t>(p.num_terms());
+  const auto W = static_cast<py::ssize_t>(p.words());
+  py::array_t<std::uint64_t> x({T, W}), z({T, W});
+  if (T * W) {
+    std::memcpy(x.mutable_data(), p.x_words().data(), T * W * 8);
+    std::memcpy(z.mutable_data(), p.z_words().data(), T * W * 8);
+  }
+  return py::make_tuple(x, z, coeff_array(p.coeffs()));
+}
+
 PYBIND11_MODULE(_wolfgang_core, m) {
   m.doc() = "B200 (sm_100a) packed-Pauli kernels behind the wolfgang_quantum API";
 
@@ -605,30 +628,15 @@ PYBIND11_MODULE(_wolfgang_core, m) {
             return translate([&] { return PauliSum::from_sparse_list(t, nonneg(n, "num_qubits")); });
           },
           py::arg("triples"), py::arg("num_qubits"))
-      .def_static(
-          "_from_packed",
-          [](long long n, py::array_t<std::uint64_t, py::array::c_style | py::array::forcecast> x,
-             py::array_t<std::uint64_t, py::array::c_style | py::array::forcecast> z,
-             py::array_t<std::complex<double>, py::array::c_style | py::array::forcecast> c) {
-            std::vector<std::uint64_t> vx(x.data(), x.data() + x.size()), vz(z.data(), z.data() + z.size());
-            std::vector<std::complex<double>> vc(c.data(), c.data() + c.size());
-            return translate([&] {
-              return PauliSum::from_packed(nonneg(n, "num_qubits"), std::move(vx), std::move(vz), std::move(vc));
-            });
-          },
-          py::arg("num_qubits"), py::arg("x"), py::arg("z"), py::arg("coeffs"),
-          "Build from packed words: x/z uint64 (num_terms, words), coeffs complex128 (num_terms,).")
-      .def("_packed",
-           [](const PauliSum& p) {
-             const auto T = static_cast<py::ssize_t>(p.num_terms());
-             const auto W = static_cast<py::ssize_t>(p.words());
-             py::array_t<std::uint64_t> x({T, W}), z({T, W});
-             if (T * W) {
-               std::memcpy(x.mutable_data(), p.x_words().data(), T * W * 8);
-               std::memcpy(z.mutable_data(), p.z_words().data(), T * W * 8);
-             }
-             return py::make_tuple(x, z, coeff_array(p.coeffs()));
-           })
+      .def_static("from_packed", from_packed, py::arg("num_qubits"), py::arg("x"), py::arg("z"), py::arg("coeffs"),
+                  "Build from packed words: x/z uint64 (num_terms, words), bit q of word q // 64 for qubit q;\n"
+                  "coeffs complex128 (num_terms,).  No labels are parsed; unused high bits of the last\n"
+                  "word must be zero.  (An addition: the reference builds only from labels or sparse lists.)")
+      .def_static("_from_packed", from_packed, py::arg("num_qubits"), py::arg("x"), py::arg("z"), py::arg("coeffs"))
+      .def("to_packed", to_packed,
+           "The packed words and coefficients: (x, z) uint64 arrays (num_terms, words) and a complex128\n"
+           "array (num_terms,), copies of the storage.")
+      .def("_packed", to_packed)
       .def_property_readonly("num_qubits", &PauliSum::num_qubits)
       .def_property_readonly("num_terms", &PauliSum::num_terms)
       .def(
