@@ -242,22 +242,36 @@ __global__ void pbatch_keep_kernel(const uint32_t* __restrict__ seg_pair, const 
 }
 
 // Survivor s of pair p goes to output slot seg_base[p] + its rank in the pair.
+// WT = W for 1 or 2 mask words (16-byte loads and stores), 0 for any width.
+template <int WT>
 __global__ void pbatch_write_kernel(const PairNum* __restrict__ pairs, const uint32_t* __restrict__ seg_pair,
                                     const uint64_t* __restrict__ seg_keys, const double* __restrict__ segsum,
                                     const uint32_t* __restrict__ keep, const uint32_t* __restrict__ pos, size_t S,
-                                    int W, uint64_t* __restrict__ ox, uint64_t* __restrict__ oz,
+                                    int Wrt, uint64_t* __restrict__ ox, uint64_t* __restrict__ oz,
                                     double* __restrict__ oc) {
+  const int W = WT > 0 ? WT : Wrt;
   for (size_t s = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; s < S;
        s += static_cast<size_t>(gridDim.x) * blockDim.x) {
     if (!keep[s]) continue;
     const uint64_t base = pairs[seg_pair[s]].seg_base;
     const size_t o = base + (pos[s] - pos[base]);
-    for (int w = 0; w < W; ++w) {
-      ox[o * W + w] = seg_keys[s * (2 * W) + w];
-      oz[o * W + w] = seg_keys[s * (2 * W) + W + w];
+    const double2 c = reinterpret_cast<const double2*>(segsum)[s];
+    if constexpr (WT == 1) {
+      const ulonglong2 k = reinterpret_cast<const ulonglong2*>(seg_keys)[s];
+      ox[o] = k.x;
+      oz[o] = k.y;
+    } else if constexpr (WT == 2) {
+      const ulonglong2 kx = reinterpret_cast<const ulonglong2*>(seg_keys)[2 * s];
+      const ulonglong2 kz = reinterpret_cast<const ulonglong2*>(seg_keys)[2 * s + 1];
+      reinterpret_cast<ulonglong2*>(ox)[o] = kx;
+      reinterpret_cast<ulonglong2*>(oz)[o] = kz;
+    } else {
+      for (int w = 0; w < W; ++w) {
+        ox[o * W + w] = seg_keys[s * (2 * W) + w];
+        oz[o * W + w] = seg_keys[s * (2 * W) + W + w];
+      }
     }
-    oc[2 * o] = segsum[2 * s];
-    oc[2 * o + 1] = segsum[2 * s + 1];
+    reinterpret_cast<double2*>(oc)[o] = c;
   }
 }
 
@@ -431,11 +445,11 @@ void run_batch(wg_products_batch_s& b, cudaStream_t s) {
   wg::check_launch("launch batch cull");
   wgs::exclusive_scan_ws<uint32_t>(b.keep.as<uint32_t>(), b.pos.as<uint32_t>(), S, b.pos.as<uint32_t>() + S,
                                    b.scan_ws.as<uint32_t>(), s);
+  auto* write = b.W == 1 ? pbatch_write_kernel<1> : b.W == 2 ? pbatch_write_kernel<2> : pbatch_write_kernel<0>;
   WG_TIMED("pbatch_write_kernel", s,
-    pbatch_write_kernel<<<g, kThreads, 0, s>>>(b.pairs.as<PairNum>(), b.seg_pair.as<uint32_t>(),
-                                               b.seg_keys.as<uint64_t>(), b.segsum.as<double>(), b.keep.as<uint32_t>(),
-                                               b.pos.as<uint32_t>(), S, b.W, b.out_x.as<uint64_t>(),
-                                               b.out_z.as<uint64_t>(), b.out_c.as<double>()));
+    write<<<g, kThreads, 0, s>>>(b.pairs.as<PairNum>(), b.seg_pair.as<uint32_t>(), b.seg_keys.as<uint64_t>(),
+                                 b.segsum.as<double>(), b.keep.as<uint32_t>(), b.pos.as<uint32_t>(), S, b.W,
+                                 b.out_x.as<uint64_t>(), b.out_z.as<uint64_t>(), b.out_c.as<double>()));
   wg::check_launch("launch batch write-out");
   pbatch_counts_kernel<<<wg::grid_for(b.n_pairs, kThreads, device, 1), kThreads, 0, s>>>(
       b.pairs.as<PairNum>(), b.pos.as<uint32_t>(), b.n_pairs, b.counts.as<uint64_t>());
