@@ -437,6 +437,25 @@ def test_large_host_operands_through_staging(oracle, op):
         assert np.ascontiguousarray(g).tobytes() == np.ascontiguousarray(w).tobytes()
 
 
+@pytest.mark.parametrize("n", [0, 20])
+def test_large_host_result_narrow_words(oracle, n):
+    """The large-result path with no mask words (0 qubits: only the
+    coefficient vector is filled) and with one word: raw products of 4,096 x
+    1,100 terms (4.5e6 terms, 72 MB of coefficients) equal the oracle."""
+    from tests.conftest import random_operator
+
+    rng = np.random.default_rng(642 + n)
+    A = random_operator(rng, n, 4096, 0.3)
+    B = random_operator(rng, n, 1100, 0.3)
+    hA = PauliSum.from_packed(n, A[1], A[2], A[3])
+    hB = PauliSum.from_packed(n, B[1], B[2], B[3])
+    got = hA.matmul(hB, simplify=False, max_intermediate_terms=4096 * 1100).to_packed()
+    want = oracle.matmul(n, A[1:], B[1:], simplify=False)
+    assert len(got[2]) * 16 > 64 << 20
+    for g, w in zip(got, want):
+        assert np.ascontiguousarray(g).tobytes() == np.ascontiguousarray(w).tobytes()
+
+
 @pytest.mark.parametrize("simplify", [True, False])
 def test_large_host_result_through_public_matmul(oracle, simplify):
     """A host result above 64 MB takes the large-result path (storage reserved,
