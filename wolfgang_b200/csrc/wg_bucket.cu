@@ -570,8 +570,9 @@ __global__ void __launch_bounds__(1024) bucket_plan_kernel(const unsigned* __res
                                                            const uint64_t* __restrict__ split, int total, bool dense0,
                                                            int thr_mode, double atol, double rtol, double thr_fixed,
                                                            unsigned favg, Control* ctl, uint32_t* __restrict__ fine_base,
-                                                           int* __restrict__ Lj) {
+                                                           int* __restrict__ Lj, uint32_t* __restrict__ order) {
   __shared__ unsigned warp_tmp[33];
+  __shared__ uint64_t by_size[kCoarseMax];
   unsigned carry = 0;
   for (int j0 = 0; j0 < B1; j0 += blockDim.x) {
     const int j = j0 + threadIdx.x;
@@ -589,6 +590,27 @@ __global__ void __launch_bounds__(1024) bucket_plan_kernel(const unsigned* __res
     if (j < B1) fine_base[j] = carry + ex;
     carry += tot;
   }
+  // The fine pass takes its coarse buckets largest first (a persistent CTA
+  // per ticket): the last tickets are the shortest jobs, which shortens the
+  // pass's tail.  B1 is a power of two.
+  for (int j = threadIdx.x; j < B1; j += blockDim.x)
+    by_size[j] = (static_cast<uint64_t>(~min(fill[j], capc)) << 32) | static_cast<uint32_t>(j);
+  __syncthreads();
+  for (int size = 2; size <= B1; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < B1 / 2; i += blockDim.x) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const uint64_t x = by_size[lo], y = by_size[hi];
+        if (((lo & size) == 0) ? (y < x) : (x < y)) {
+          by_size[lo] = y;
+          by_size[hi] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int j = threadIdx.x; j < B1; j += blockDim.x) order[j] = static_cast<uint32_t>(by_size[j]);
   if (threadIdx.x == 0) {
     fine_base[B1] = carry;
     ctl->fine_total = carry;
@@ -623,6 +645,7 @@ struct FineParams {
   Control* ctl;
   unsigned favg;              // target items per fine bucket
   int trace;                  // record per-phase cycles
+  const uint32_t* order;      // [B1] coarse buckets, largest first (ticket -> bucket)
 };
 
 // Exclusive block scans (blockDim.x a multiple of 32, at most 1024; tmp holds
@@ -759,9 +782,10 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     if (P.trace && threadIdx.x == 0) s_tp[0] = clock64();
     if (threadIdx.x == 0) s_job = atomicAdd(&P.ctl->k2_ticket, 1u);
     __syncthreads();
-    const int j = static_cast<int>(s_job);
+    const int ticket = static_cast<int>(s_job);
     __syncthreads();
-    if (j >= P.B1) break;
+    if (ticket >= P.B1) break;
+    const int j = static_cast<int>(P.order[ticket]);
     const uint32_t n = min(P.fill[j], P.capc);
     const size_t base = static_cast<size_t>(j) * P.capc;
     const size_t rbase = static_cast<size_t>(j) * P.rstride;
@@ -1816,9 +1840,10 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   }
   uint32_t* fine_base = ws.take_as<uint32_t>(B1 + 1);
   int* Lj = ws.take_as<int>(B1);
+  uint32_t* order = ws.take_as<uint32_t>(B1);
   WG_TIMED("bucket_plan_kernel", s,
     bucket_plan_kernel<<<1, 1024, 0, s>>>(fill, B1, capc, split, total, dense0, thr.mode, thr.atol, thr.rtol,
-                                          thr.fixed, favg, dctl, fine_base, Lj));
+                                          thr.fixed, favg, dctl, fine_base, Lj, order));
   wg::check_launch("launch bucket plan");
   stamp("coarse");
 
@@ -1831,7 +1856,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   {
     uint16_t* fid_tmp = ws.take_as<uint16_t>(region);
     const FineParams fp{fill, capc, B1, total, fine_base, Lj, idx1, fid_tmp, rstride, rec_code, rec_idx,
-                        fine_start, fine_count, fine_L, dctl, favg, trace ? 1 : 0};
+                        fine_start, fine_count, fine_L, dctl, favg, trace ? 1 : 0, order};
     auto* k2 = bucket_fine_kernel<KW, Src>;
     set_smem(k2, kK2Smem);
     int per_sm = 0;
