@@ -1803,7 +1803,7 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   // every intermediate lives in the device workspace
   using WS = wg::Workspace;
   const size_t ws_bytes = WS::rounded(sizeof(Control)) + WS::rounded(8 * B1) + WS::rounded(4 * B1) +
-                          WS::rounded(4 * region) + WS::rounded(4 * (B1 + 1)) + WS::rounded(4 * B1) +
+                          WS::rounded(4 * region) + WS::rounded(4 * (B1 + 1)) + 2 * WS::rounded(4 * B1) +
                           WS::rounded(8 * records) + WS::rounded(4 * records) + 2 * WS::rounded(4 * Gmax) +
                           WS::rounded(2 * Gmax) + WS::rounded(2 * region) + WS::rounded(8 * records) +
                           2 * WS::rounded(4 * Gmax) + WS::rounded(4);
