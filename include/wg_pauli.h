@@ -269,6 +269,15 @@ int wg_last_sort_algorithm(void);
  * target means fewer, fuller buckets.  Accepts 0 or 32..2048. */
 int wg_set_bucket_fine_target(unsigned items);
 
+/* Layout of WG_SORT_BUCKET's fine partition (process-wide).  1 (the default):
+ * every fine bucket owns room for 2048 records and the partition pass writes
+ * each item as it counts it, where that room (20 bytes a record) takes at
+ * most a quarter of the device's memory; a coarse bucket with a fine bucket
+ * over 2048 items is packed in a second pass.  0: always count first, then
+ * pack (less memory).  Both give identical results.  No reference
+ * counterpart; a tuning setting.  Accepts 0 or 1. */
+int wg_set_bucket_one_pass(int on);
+
 /* -------------------------------------------------------- expectation ---- */
 /* <psi|H|psi> (PauliSum::expectation_statevector_complex{128,64},
  * include/wolfgang/pauli_sum.hpp:91-94; DevicePauliSum::expectation_statevector_*

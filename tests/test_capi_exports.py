@@ -94,6 +94,14 @@ def test_bucket_fine_target_is_range_checked_before_device_work():
     capi.set_bucket_fine_target(0)
 
 
+def test_bucket_one_pass_setting_is_checked():
+    for bad in (-1, 2):
+        rc = capi.lib().wg_set_bucket_one_pass(bad)
+        assert rc == capi.WG_ERR_INVALID and b"one-pass" in capi.lib().wg_last_error()
+    capi.set_bucket_one_pass(False)
+    capi.set_bucket_one_pass(True)
+
+
 def test_chunked_download_needs_a_callback():
     L = capi.lib()
     rc = L.wg_memcpy_dtoh_chunked(0, None, 64, None, None, None)

@@ -185,6 +185,45 @@ def test_bucket_fine_buckets_split_again(cuda, oracle, algo, monkeypatch, capfd,
     assert same(got, oracle.simplify(40, x, z, c))
 
 
+@pytest.mark.parametrize("one_pass", [True, False])
+@pytest.mark.parametrize("case", ["klocal100", "dup40", "refine"])
+def test_bucket_fine_layouts_identical(cuda, oracle, algo, monkeypatch, capfd, one_pass, case):
+    """The fine partition written in one pass (every fine bucket owns 2048
+    record slots) and in two passes (count, then pack) give the oracle's bits:
+    k-local products, a duplicate-heavy simplify, and a fine target near
+    capacity whose overfull fine buckets send their coarse buckets to the
+    packed second pass and to refinement."""
+    import re
+
+    rng = seeded("fine-layout", case)
+    algo(capi.WG_SORT_BUCKET)
+    capi.set_bucket_one_pass(one_pass)
+    try:
+        if case == "klocal100":
+            A, B = klocal(rng, 100, 2048), klocal(rng, 100, 1024)
+            got = G.products(100, A[1:], B[1:])
+            want = oracle.simplify(100, *oracle.matmul(100, A[1:], B[1:], simplify=False), 1e-12, 0.0)
+        elif case == "dup40":
+            _, x, z, c = random_operator(rng, 40, 1_200_000, 0.25, 300_000)
+            got = G.simplify(40, x, z, c)
+            want = oracle.simplify(40, x, z, c)
+        else:
+            _, x, z, c = random_operator(rng, 40, 400_000, 0.25, 150_000)
+            monkeypatch.setenv("WG_BUCKET_TRACE", "1")
+            capi.set_bucket_fine_target(1800)
+            try:
+                got = G.simplify(40, x, z, c)
+            finally:
+                capi.set_bucket_fine_target(0)
+            refined = [int(v) for v in re.findall(r"refined=(\d+)", capfd.readouterr().err)]
+            assert refined and refined[-1] > 0
+            want = oracle.simplify(40, x, z, c)
+        assert capi.last_sort_algorithm() == capi.WG_SORT_BUCKET
+    finally:
+        capi.set_bucket_one_pass(True)
+    assert same(got, want)
+
+
 def test_bucket_fine_target_rejects_out_of_range(cuda):
     for bad in (1, 31, 2049):
         with pytest.raises(capi.WGInvalid):

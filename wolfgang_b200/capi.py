@@ -85,6 +85,7 @@ _SIGNATURES: dict[str, list] = {
     "wg_set_sort_algorithm": [_i],
     "wg_last_sort_algorithm": [],
     "wg_set_bucket_fine_target": [ctypes.c_uint],
+    "wg_set_bucket_one_pass": [ctypes.c_int],
     "wg_expect_plan_create": [_i, _sz, _sz, _vp, _vp, _vp, _pvp, _vp],
     "wg_expect_plan_destroy": [_vp],
     "wg_expect_plan_set_coeffs": [_vp, _vp, _vp],
@@ -183,6 +184,11 @@ _sort_setting = [WG_SORT_AUTO]
 def set_bucket_fine_target(items: int) -> None:
     """Target items per fine bucket of the bucketed sort (0: the default, 896); results do not change."""
     check(lib().wg_set_bucket_fine_target(int(items)))
+
+
+def set_bucket_one_pass(on: bool) -> None:
+    """Bucketed sort: fine partition written in one pass where memory allows (True, the default), or two."""
+    check(lib().wg_set_bucket_one_pass(1 if on else 0))
 
 
 def autotune_mode(mode: int | None = None) -> int:

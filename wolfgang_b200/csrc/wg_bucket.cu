@@ -636,8 +636,8 @@ struct FineParams {
   const int* Lj;              // prefix | dense << 16
   const uint32_t* idx_in;     // [B1][capc]
   uint16_t* fid_tmp;          // [B1][capc] fine bucket of each item
-  uint32_t rstride;           // record region per coarse bucket (multiple of 32)
-  uint64_t* rec_code;         // [B1][rstride] in fine-bucket order, buckets 32-aligned
+  uint32_t rstride;           // record region per coarse bucket (multiple of 32); 0: one-pass layout
+  uint64_t* rec_code;         // records in fine-bucket order (see bucket_fine_kernel)
   uint32_t* rec_idx;
   uint32_t* fine_start;       // [G]
   uint32_t* fine_count;       // [G] count | kExactBit | kPureBit
@@ -777,6 +777,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
   __shared__ unsigned s_nfix;
   __shared__ int s_fixf[kRefineMax];
   __shared__ uint64_t s_fixv[kRefineMax];
+  __shared__ int s_over;  // one-pass layout: a fine bucket got more than kCap items
   const int total = P.total;
   while (true) {
     if (P.trace && threadIdx.x == 0) s_tp[0] = clock64();
@@ -788,7 +789,14 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     const int j = static_cast<int>(P.order[ticket]);
     const uint32_t n = min(P.fill[j], P.capc);
     const size_t base = static_cast<size_t>(j) * P.capc;
-    const size_t rbase = static_cast<size_t>(j) * P.rstride;
+    // One-pass layout (rstride 0): fine slot f of this coarse bucket owns
+    // records [(fine_base[j] + f) * kCap, + kCap), and pass 1 writes every item
+    // there as it counts it; a coarse bucket with a fine bucket over kCap
+    // items falls back to the two passes, packing its fine buckets 32-aligned
+    // from the start of its region (slots * kCap records: room enough).
+    // Otherwise each coarse bucket owns rstride records, packed the same way.
+    const bool one_pass = P.rstride == 0;
+    const size_t rbase = one_pass ? static_cast<size_t>(P.fine_base[j]) * kCap : static_cast<size_t>(j) * P.rstride;
     const uint32_t g0 = P.fine_base[j];
     const int slots = static_cast<int>(P.fine_base[j + 1] - g0);
     const int target = static_cast<int>(fine_target(n, P.favg));
@@ -900,20 +908,33 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     for (int f = threadIdx.x; f < slots; f += blockDim.x) cnt[f] = 0;
     build_top_table(fs, s_ns, ftop);
     __syncthreads();
-    // pass 1: fine bucket of every item
+    // pass 1: fine bucket of every item; in the one-pass layout also its
+    // record (code relative to the fine prefix, index) at its fine slot
     for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
       const uint32_t t = t0 + threadIdx.x;
-      const bool valid = t < n;
-      int f = 0;
-      if (valid) {
+      if (t < n) {
+        const uint32_t p = P.idx_in[base + t];
         uint64_t c[KW];
-        src.ckey(P.idx_in[base + t], c);
-        f = upper_bound_top(fs, ftop, code_of<KW>(c, Lp, densep));
+        src.ckey(p, c);
+        const int f = upper_bound_top(fs, ftop, code_of<KW>(c, Lp, densep));
         P.fid_tmp[base + t] = static_cast<uint16_t>(f);
+        const unsigned slot = atomicAdd(&cnt[f], 1u);
+        if (one_pass && slot < static_cast<unsigned>(kCap)) {
+          const int Lf = fL[f];
+          const size_t r = rbase + static_cast<size_t>(f) * kCap + slot;
+          P.rec_code[r] = code_of<KW>(c, Lf & 0xffff, (Lf >> 16) & 1);
+          P.rec_idx[r] = p;
+        }
       }
-      if (valid) atomicAdd(&cnt[f], 1u);
+    }
+    if (threadIdx.x == 0) s_over = 0;
+    __syncthreads();
+    if (one_pass) {
+      for (int f = threadIdx.x; f < slots; f += blockDim.x)
+        if (cnt[f] > static_cast<unsigned>(kCap)) s_over = 1;
     }
     __syncthreads();
+    const bool placed = one_pass && s_over == 0;
     // Refinement.  The sample puts about 2.5 times the mean into the largest of
     // a million fine buckets; one over kCap items whose range holds more than
     // one code gets one more splitter from its own samples (refine_splitter),
@@ -991,43 +1012,56 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
       __syncthreads();
     }
     if (P.trace && threadIdx.x == 0) s_tp[3] = clock64();
-    // fine bucket offsets, each bucket starting on a multiple of 32 records
-    // (slots <= kFineSlots: a few rounds of the block scan)
-    unsigned carry = 0;
-    for (int f0 = 0; f0 < slots; f0 += blockDim.x) {
-      const int f = f0 + threadIdx.x;
-      const unsigned c = f < slots ? cnt[f] : 0u;
-      unsigned tot;
-      const unsigned ex = block_exclusive_scan((c + 31u) & ~31u, warp_tmp, &tot);
-      if (f < slots) {
-        const unsigned off = carry + ex;
+    if (placed) {
+      // every record is in place: fine bucket f starts at its slot
+      for (int f = threadIdx.x; f < slots; f += blockDim.x) {
         const bool exact = (fL[f] >> 16) & 1;
         const bool pure = exact && (fL[f] & 0xffff) == total;  // every key of the bucket is equal
-        P.fine_start[g0 + f] = static_cast<uint32_t>(rbase + off);
-        P.fine_count[g0 + f] = c | (exact ? kExactBit : 0u) | (pure ? kPureBit : 0u);
+        P.fine_start[g0 + f] = static_cast<uint32_t>(rbase + static_cast<size_t>(f) * kCap);
+        P.fine_count[g0 + f] = cnt[f] | (exact ? kExactBit : 0u) | (pure ? kPureBit : 0u);
         P.fine_L[g0 + f] = static_cast<uint16_t>(fL[f] & 0xffff);
-        cnt[f] = off;
       }
-      carry += tot;
-    }
-    __syncthreads();
-    if (P.trace && threadIdx.x == 0) s_tp[4] = clock64();
-    // pass 2: (code relative to the fine prefix, index) into fine-bucket order
-    for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
-      const uint32_t t = t0 + threadIdx.x;
-      const bool valid = t < n;
-      const int f = valid ? P.fid_tmp[base + t] : 0;
-      const unsigned pos = valid ? atomicAdd(&cnt[f], 1u) : 0u;
-      if (valid) {
-        const uint32_t p = P.idx_in[base + t];
-        uint64_t c[KW];
-        src.ckey(p, c);
-        const int Lf = fL[f];
-        P.rec_code[rbase + pos] = code_of<KW>(c, Lf & 0xffff, (Lf >> 16) & 1);
-        P.rec_idx[rbase + pos] = p;
+      __syncthreads();
+      if (P.trace && threadIdx.x == 0) s_tp[4] = clock64();
+    } else {
+      // fine bucket offsets, each bucket starting on a multiple of 32 records
+      // (slots <= kFineSlots: a few rounds of the block scan)
+      unsigned carry = 0;
+      for (int f0 = 0; f0 < slots; f0 += blockDim.x) {
+        const int f = f0 + threadIdx.x;
+        const unsigned c = f < slots ? cnt[f] : 0u;
+        unsigned tot;
+        const unsigned ex = block_exclusive_scan((c + 31u) & ~31u, warp_tmp, &tot);
+        if (f < slots) {
+          const unsigned off = carry + ex;
+          const bool exact = (fL[f] >> 16) & 1;
+          const bool pure = exact && (fL[f] & 0xffff) == total;  // every key of the bucket is equal
+          P.fine_start[g0 + f] = static_cast<uint32_t>(rbase + off);
+          P.fine_count[g0 + f] = c | (exact ? kExactBit : 0u) | (pure ? kPureBit : 0u);
+          P.fine_L[g0 + f] = static_cast<uint16_t>(fL[f] & 0xffff);
+          cnt[f] = off;
+        }
+        carry += tot;
       }
+      __syncthreads();
+      if (P.trace && threadIdx.x == 0) s_tp[4] = clock64();
+      // pass 2: (code relative to the fine prefix, index) into fine-bucket order
+      for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        const bool valid = t < n;
+        const int f = valid ? P.fid_tmp[base + t] : 0;
+        const unsigned pos = valid ? atomicAdd(&cnt[f], 1u) : 0u;
+        if (valid) {
+          const uint32_t p = P.idx_in[base + t];
+          uint64_t c[KW];
+          src.ckey(p, c);
+          const int Lf = fL[f];
+          P.rec_code[rbase + pos] = code_of<KW>(c, Lf & 0xffff, (Lf >> 16) & 1);
+          P.rec_idx[rbase + pos] = p;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
     if (P.trace && threadIdx.x == 0) {
       s_tp[5] = clock64();
       for (int q = 0; q < 5; ++q) atomicAdd(&P.ctl->fphase[q], static_cast<unsigned long long>(s_tp[q + 1] - s_tp[q]));
@@ -1658,6 +1692,7 @@ __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParam
 
 std::atomic<int> g_sort_algorithm{WG_SORT_AUTO};
 std::atomic<unsigned> g_fine_target{0};  // target items per fine bucket; 0: kFineAvg
+std::atomic<bool> g_one_pass_fine{true};  // fine pass in one-pass layout where it fits (see run_bucket)
 thread_local unsigned t_fine_choice = 0;   // the autotuner's target for the running call; 0: none
 
 // Fine-bucket targets the autotuner chooses among (kFineAvg is candidate 2).
@@ -1795,9 +1830,16 @@ bool run_bucket(int device, const Src& src, uint32_t n, int total, const ThrSpec
   // bucket starting on a multiple of 32
   const uint64_t rstride64 = ((static_cast<uint64_t>(capc) + 31) & ~uint64_t{31}) + 32ull * kFineSlots;
   if (static_cast<uint64_t>(B1) * rstride64 >= 0xffffffffull) return false;
-  const uint32_t rstride = static_cast<uint32_t>(rstride64);
-  const size_t records = static_cast<size_t>(B1) * rstride;
   const auto& props = wg::device_props(device);
+  // One-pass layout (kCap records per fine slot, the fine pass writes each
+  // item as it counts it) where its 20 bytes per record fit in a quarter of
+  // the device's memory and record indices stay 32-bit; else rstride records
+  // per coarse bucket and two passes.
+  const uint64_t one_records = static_cast<uint64_t>(Gmax) * kCap;
+  const bool one_pass = g_one_pass_fine.load(std::memory_order_relaxed) && one_records < 0xffffffffull &&
+                        one_records * 20 <= props.total_mem / 4;
+  const uint32_t rstride = one_pass ? 0u : static_cast<uint32_t>(rstride64);
+  const size_t records = one_pass ? static_cast<size_t>(one_records) : static_cast<size_t>(B1) * rstride64;
   const bool trace = stamp.on;
 
   // every intermediate lives in the device workspace
@@ -2095,6 +2137,13 @@ int wg_set_bucket_fine_target(unsigned items) {
     if (items != 0 && (items < 32 || items > static_cast<unsigned>(kCap)))
       wg::throw_invalid("fine bucket target must be 0 (default) or between 32 and 2048 items");
     g_fine_target.store(items, std::memory_order_relaxed);
+  });
+}
+
+int wg_set_bucket_one_pass(int on) {
+  return wg::guarded([&] {
+    if (on != 0 && on != 1) wg::throw_invalid("one-pass setting must be 0 or 1");
+    g_one_pass_fine.store(on != 0, std::memory_order_relaxed);
   });
 }
 

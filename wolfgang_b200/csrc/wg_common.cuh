@@ -92,6 +92,7 @@ struct DeviceProps {
   int sm_count = 0;
   int max_smem_optin = 0;
   size_t l2_bytes = 0;
+  size_t total_mem = 0;
 };
 const DeviceProps& device_props(int device);
 int current_device();

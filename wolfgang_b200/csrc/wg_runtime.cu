@@ -102,6 +102,9 @@ const DeviceProps& device_props(int device) {
     p.max_smem_optin = v;
     check_cuda(cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, device), "query L2 size");
     p.l2_bytes = static_cast<size_t>(v);
+    cudaDeviceProp dp{};
+    check_cuda(cudaGetDeviceProperties(&dp, device), "query device memory");
+    p.total_mem = dp.totalGlobalMem;
   }
   if (!g_pool_ready[device]) {
     // Keep freed blocks cached in the pool instead of returning them to the
