@@ -54,6 +54,7 @@ constexpr int kPiece = 8;                // terms per adjoint table
 constexpr int kQuadTerms = 4 * kPiece;   // terms per adjoint quad (four tables)
 constexpr int kAdjR = 16;                // outputs per thread in the adjoint
 constexpr int kAdjTileLog = 12;          // outputs per adjoint item: 2^12
+constexpr int kAdjQuadChunk = 2048;      // quads whose tile sign masks a CTA stages at a time
 constexpr uint32_t kDiagFlag = 4;        // ty bit: the term's group has x == 0
 
 enum SubKind : uint32_t { kDiag = 0, kLowX = 1, kHighX = 2 };
@@ -106,13 +107,14 @@ struct PlanDev {
   double* td;                // [2T] sorted c_k * i^y
   double* table;             // [2 * entries] adjoint tables
   double* partial;           // forward partial sums
+  uint32_t* stid;            // [Q][256] adjoint: bit kk = parity(z_kk & l) for lane offset l
 };
 
 struct wg_plan_host {
   int device;
   PlanDev dev;
   size_t n_groups = 0;
-  wg::Scratch blob, coeffs, td, table, partial;
+  wg::Scratch blob, coeffs, td, table, partial, stid;
 };
 
 }  // namespace
@@ -391,6 +393,7 @@ __global__ void __launch_bounds__(kThreads) expect_total_kernel(BatchDev B) {
 template <typename Amp>
 __global__ void __launch_bounds__(kThreads) expect_adjoint_kernel(BatchDev B) {
   __shared__ unsigned long long s_item;
+  __shared__ uint32_t s_hi[kAdjQuadChunk];  // per quad of the chunk: parity(z & (hi ^ x)) masks
   const int tid = threadIdx.x;
   while (true) {
     if (tid == 0) s_item = atomicAdd(B.counters + 1, 1ull);
@@ -405,50 +408,70 @@ __global__ void __launch_bounds__(kThreads) expect_adjoint_kernel(BatchDev B) {
     const int tlog = P.n < kAdjTileLog ? P.n : kAdjTileLog;
     const uint64_t TS = uint64_t{1} << tlog;
     const int R = TS >= kThreads ? static_cast<int>(TS / kThreads) : 1;
-    if (static_cast<uint64_t>(tid) >= TS) continue;
-    const uint64_t j0 = (item - B.tile_base[p]) * TS + tid;
+    const bool active = static_cast<uint64_t>(tid) < TS;
+    // b = j0 ^ x splits into the tile's bits and the lane's: j0 = hi + tid
+    // with hi a multiple of TS (>= 256 or 0), so a term's sign parity(z & b)
+    // is parity(z & (hi ^ x)) -- staged per quad by the CTA, once per tile --
+    // XOR parity(z & tid), the plan's stid table.
+    const uint64_t hi = (item - B.tile_base[p]) * TS;
+    const uint64_t j0 = hi + tid;
     c128 acc[kAdjR];
 #pragma unroll
     for (int r = 0; r < kAdjR; ++r) acc[r] = {0.0, 0.0};
     const double2* tab = reinterpret_cast<const double2*>(P.table);
-    for (uint32_t qi = 0; qi < P.Q; ++qi) {
-      const QuadDev* qd = P.quad + qi;  // read in place: its small arrays are indexed at run time
-      const uint32_t nk = qd->nk, t0 = qd->t0;
-      uint64_t b = j0 ^ qd->x;
-      uint32_t S = 0;
-      for (uint32_t kk = 0; kk < nk; ++kk) S |= static_cast<uint32_t>(__popcll(P.tz[t0 + kk] & b) & 1) << kk;
-      const int np = static_cast<int>((nk + kPiece - 1) / kPiece);
-      uint32_t pl[4], tb[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        pl[q] = qd->plane[q];
-        tb[q] = qd->tbase[q];
+    for (uint32_t q0 = 0; q0 < P.Q; q0 += kAdjQuadChunk) {
+      const uint32_t qn = min(static_cast<uint32_t>(kAdjQuadChunk), P.Q - q0);
+      __syncthreads();  // the previous chunk's masks are read
+      for (uint32_t qq = tid; qq < qn; qq += kThreads) {
+        const QuadDev* qd = P.quad + q0 + qq;
+        const uint64_t hb = hi ^ qd->x;
+        const uint32_t nk = qd->nk, t0 = qd->t0;
+        uint32_t m = 0;
+        for (uint32_t kk = 0; kk < nk; ++kk) m |= static_cast<uint32_t>(__popcll(P.tz[t0 + kk] & hb) & 1) << kk;
+        s_hi[qq] = m;
       }
+      __syncthreads();
+      if (!active) continue;
+      for (uint32_t qq = 0; qq < qn; ++qq) {
+        const uint32_t qi = q0 + qq;
+        const QuadDev* qd = P.quad + qi;  // read in place: its small arrays are indexed at run time
+        const uint32_t nk = qd->nk;
+        uint64_t b = j0 ^ qd->x;
+        uint32_t S = s_hi[qq] ^ P.stid[static_cast<size_t>(qi) * kThreads + tid];
+        const int np = static_cast<int>((nk + kPiece - 1) / kPiece);
+        uint32_t pl[4], tb[4];
 #pragma unroll
-      for (int r = 0; r < kAdjR; ++r) {
-        if (r < R) {
-          if (r > 0) {
-            // Gray step flips output bit 8 + ctz(r), and the same bit of b
-            const int j = (r & 1) ? 0 : (r & 2) ? 1 : (r & 4) ? 2 : 3;
-            b ^= uint64_t{1} << (8 + j);
-            S ^= pl[j];
-          }
-          const double2 f0 = tab[tb[0] + (S & 0xffu)];
-          double fre = f0.x, fim = f0.y;
+        for (int q = 0; q < 4; ++q) {
+          pl[q] = qd->plane[q];
+          tb[q] = qd->tbase[q];
+        }
 #pragma unroll
-          for (int pc = 1; pc < 4; ++pc) {
-            if (pc < np) {
-              const double2 f = tab[tb[pc] + ((S >> (kPiece * pc)) & 0xffu)];
-              fre += f.x;
-              fim += f.y;
+        for (int r = 0; r < kAdjR; ++r) {
+          if (r < R) {
+            if (r > 0) {
+              // Gray step flips output bit 8 + ctz(r), and the same bit of b
+              const int j = (r & 1) ? 0 : (r & 2) ? 1 : (r & 4) ? 2 : 3;
+              b ^= uint64_t{1} << (8 + j);
+              S ^= pl[j];
             }
+            const double2 f0 = tab[tb[0] + (S & 0xffu)];
+            double fre = f0.x, fim = f0.y;
+#pragma unroll
+            for (int pc = 1; pc < 4; ++pc) {
+              if (pc < np) {
+                const double2 f = tab[tb[pc] + ((S >> (kPiece * pc)) & 0xffu)];
+                fre += f.x;
+                fim += f.y;
+              }
+            }
+            const c128 v = load_amp<Amp>(psi, b);
+            acc[r].re += v.re * fre - v.im * fim;
+            acc[r].im += v.re * fim + v.im * fre;
           }
-          const c128 v = load_amp<Amp>(psi, b);
-          acc[r].re += v.re * fre - v.im * fim;
-          acc[r].im += v.re * fim + v.im * fre;
         }
       }
     }
+    if (!active) continue;
     uint64_t j = j0;
 #pragma unroll
     for (int r = 0; r < kAdjR; ++r) {
@@ -461,6 +484,19 @@ __global__ void __launch_bounds__(kThreads) expect_adjoint_kernel(BatchDev B) {
 }
 
 // ------------------------------------------------------------- plan build
+
+// stid[q][l] bit kk = parity(z_kk & l) over the terms of quad q, for the
+// adjoint's lane offsets l < 256 (z-masks only: built once per plan).
+__global__ void plan_stid_kernel(PlanDev P) {
+  const uint32_t l = threadIdx.x;
+  for (uint32_t q = blockIdx.x; q < P.Q; q += gridDim.x) {
+    const QuadDev* qd = P.quad + q;
+    const uint32_t nk = qd->nk, t0 = qd->t0;
+    uint32_t m = 0;
+    for (uint32_t kk = 0; kk < nk; ++kk) m |= static_cast<uint32_t>(__popcll(P.tz[t0 + kk] & l) & 1) << kk;
+    P.stid[static_cast<size_t>(q) * kThreads + l] = m;
+  }
+}
 
 // td[i] = c[torig[i]] * i^{y_i} (sorted order).
 __global__ void plan_coeffs_kernel(PlanDev P) {
@@ -677,15 +713,21 @@ wg_plan_host* make_plan(int device, size_t n, size_t T, const uint64_t* x, const
   p->td.reset(16 * T, s);
   p->table.reset(16 * std::max<size_t>(1, table_entries), s);
   p->partial.reset(8 * std::max<uint64_t>(1, pbase), s);
+  p->stid.reset(4 * kThreads * std::max<size_t>(1, d.Q), s);
   d.td = p->td.as<double>();
   d.table = p->table.as<double>();
   d.partial = p->partial.as<double>();
+  d.stid = p->stid.as<uint32_t>();
+  if (d.Q) {
+    plan_stid_kernel<<<std::min<uint32_t>(d.Q, 65535u), kThreads, 0, s>>>(d);
+    wg::check_launch("launch adjoint lane signs");
+  }
   refresh_coeffs(*p, s);
   // pageable source above: wait until the plan image is on the device
   wg::check_cuda(cudaStreamSynchronize(s), "build plan");
   // The plan outlives the caller's stream: release its buffers on the legacy
   // default stream.
-  for (wg::Scratch* b : {&p->blob, &p->coeffs, &p->td, &p->table, &p->partial}) b->rebind(nullptr);
+  for (wg::Scratch* b : {&p->blob, &p->coeffs, &p->td, &p->table, &p->partial, &p->stid}) b->rebind(nullptr);
   return p.release();
 }
 
