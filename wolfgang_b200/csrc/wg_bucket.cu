@@ -1635,7 +1635,7 @@ struct OutputParams {
 // survivors at a time, their loads issued before any store.
 template <int KW, class Src>
 __global__ void __launch_bounds__(256) bucket_output_kernel(Src src, OutputParams P) {
-  constexpr int kU = 6;  // survivors per lane in flight (4: 7.95 ms, 6: 7.00 ms, 8: 8.44 ms at config 2)
+  constexpr int kU = 6;  // survivors per lane in flight (config 2: 4: 7.95 ms, 5: 7.19, 6: 7.03, 7: 7.14, 8: 8.44)
   const int lane = threadIdx.x & 31;
   const unsigned G = P.ctl->fine_total;
   const unsigned warps = gridDim.x * (blockDim.x >> 5);
