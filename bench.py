@@ -396,7 +396,7 @@ def bench_products(args, world, rank, torch) -> dict:
         # bucketed path: an item is a 4-byte product index; codes are 8 bytes;
         # operand gathers hit L2 and are not counted
         "bucket_coarse_kernel": P * 4,                         # write the item index
-        "bucket_fine_kernel": P * (4 + 2 + 8 + 4),             # idx in, fine id out, code + idx out (one pass)
+        "bucket_fine_kernel": P * (4 + 8 + 4),                 # idx in, code + idx out (one pass)
         "bucket_final_kernel": P * (8 + 4) + U * (4 + 16),     # code + idx in; survivors' idx + sum out
         "bucket_output_kernel": U * (4 + 16) + U * (8 * 2 * W + 16),  # survivors in, the U terms out
     }

@@ -917,7 +917,7 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
         uint64_t c[KW];
         src.ckey(p, c);
         const int f = upper_bound_top(fs, ftop, code_of<KW>(c, Lp, densep));
-        P.fid_tmp[base + t] = static_cast<uint16_t>(f);
+        if (!one_pass) P.fid_tmp[base + t] = static_cast<uint16_t>(f);
         const unsigned slot = atomicAdd(&cnt[f], 1u);
         if (one_pass && slot < static_cast<unsigned>(kCap)) {
           const int Lf = fL[f];
@@ -935,6 +935,23 @@ __global__ void __launch_bounds__(kK2Threads) bucket_fine_kernel(Src src, FinePa
     }
     __syncthreads();
     const bool placed = one_pass && s_over == 0;
+    if (one_pass && !placed) {
+      // the packed fallback needs every item's fine bucket: count again,
+      // keeping them (the one pass did not store them)
+      for (int f = threadIdx.x; f < slots; f += blockDim.x) cnt[f] = 0;
+      __syncthreads();
+      for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        if (t < n) {
+          uint64_t c[KW];
+          src.ckey(P.idx_in[base + t], c);
+          const int f = upper_bound_top(fs, ftop, code_of<KW>(c, Lp, densep));
+          P.fid_tmp[base + t] = static_cast<uint16_t>(f);
+          atomicAdd(&cnt[f], 1u);
+        }
+      }
+      __syncthreads();
+    }
     // Refinement.  The sample puts about 2.5 times the mean into the largest of
     // a million fine buckets; one over kCap items whose range holds more than
     // one code gets one more splitter from its own samples (refine_splitter),
